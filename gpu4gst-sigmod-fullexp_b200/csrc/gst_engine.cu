@@ -1,0 +1,668 @@
+// Host side of the GST engine and its C ABI (include/gst.h).
+//
+// A gst_graph owns the device CSR and a pool of query slots (state slab,
+// one-label distances, worklists).  gst_solve runs one query in slot 0;
+// gst_solve_batch runs up to cfg.max_batch queries at once in as many slots,
+// refilling a slot as soon as its query finishes.  The level loop is a fixed
+// launch sequence (sssp, ctrl, rows, ctrl, grow, ctrl) that the host issues a few
+// levels ahead of the device; every kernel reads its work counts from the
+// device-side contexts, so extra launches after a query finishes are no-ops.
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "gst.h"
+#include "gst_device.cuh"
+
+using namespace gst;
+
+namespace {
+
+thread_local std::string tl_err;
+
+struct Slot {
+  size_t rw_cap = 0;     // cells per row the slab was sized for
+  int64_t V = 0;
+  uint64_t* table = nullptr;
+  uint32_t* dist = nullptr;
+  uint32_t* rowbits = nullptr;
+  uint4* q[2] = {nullptr, nullptr};
+  uint4* far[2] = {nullptr, nullptr};
+  uint32_t* rows = nullptr;
+  int32_t* out = nullptr;
+  uint64_t* stack = nullptr;
+  uint32_t qcap = 0, farcap = 0, rowcap = 0, outcap = 0, stackcap = 0;
+  size_t bytes = 0;
+};
+
+}  // namespace
+
+struct gst_engine {
+  int device = 0;
+  gst_config cfg{};
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int sms = 148;
+  int grow_blocks = 0, sssp_blocks = 0;
+  std::string err;
+  std::mutex mu;
+};
+
+struct gst_graph {
+  gst_engine* eng = nullptr;
+  int64_t V = 0, E = 0;
+  int64_t* d_beg = nullptr;
+  int2* d_edges = nullptr;
+  std::vector<int64_t> h_beg;
+  std::vector<Slot> slots;
+  Ctx* d_ctx = nullptr;       // MAXB contexts
+  Ctx* h_ctx = nullptr;       // pinned mirror
+};
+
+struct gst_groups {
+  gst_graph* g = nullptr;
+  int32_t n = 0;
+  int64_t* d_ptr = nullptr;
+  int32_t* d_mem = nullptr;
+  std::vector<int64_t> h_ptr;
+};
+
+namespace {
+
+gst_status fail(gst_engine* e, gst_status s, const std::string& msg) {
+  if (e) e->err = msg;
+  tl_err = msg;
+  return s;
+}
+
+#define CK(call)                                                                      \
+  do {                                                                                \
+    cudaError_t _e = (call);                                                          \
+    if (_e != cudaSuccess)                                                            \
+      return fail(eng, GST_DEVICE_ERROR,                                              \
+                  std::string(#call) + ": " + cudaGetErrorString(_e));                \
+  } while (0)
+
+void free_slot(Slot& s) {
+  cudaFree(s.table);
+  cudaFree(s.dist);
+  cudaFree(s.rowbits);
+  cudaFree(s.q[0]);
+  cudaFree(s.q[1]);
+  cudaFree(s.far[0]);
+  cudaFree(s.far[1]);
+  cudaFree(s.rows);
+  cudaFree(s.out);
+  cudaFree(s.stack);
+  s = Slot();
+}
+
+// worklist capacity for a slab of V rows of rw cells
+uint32_t list_cap(int64_t V, size_t rw) {
+  const uint64_t want = (uint64_t)V * rw + 4ull * (uint64_t)V + 4096;
+  return (uint32_t)std::min<uint64_t>(want, 1ull << 26);
+}
+
+size_t slot_bytes(int64_t V, size_t rw) {
+  const uint64_t cap = list_cap(V, rw);
+  return (size_t)V * rw * 8 + (size_t)V * DIST_STRIDE * 4 + ((size_t)V + 31) / 32 * 4 +
+         4 * (size_t)cap * 16 + (size_t)V * 4 + (size_t)(1 << 16) * 12 + (size_t)(1 << 18) * 8;
+}
+
+gst_status ensure_slot(gst_engine* eng, gst_graph* g, size_t idx, size_t rw) {
+  if (g->slots.size() <= idx) g->slots.resize(idx + 1);
+  Slot& s = g->slots[idx];
+  if (s.table && s.rw_cap >= rw && s.V == g->V) return GST_OK;
+  free_slot(s);
+  const int64_t V = g->V;
+  s.V = V;
+  s.rw_cap = rw;
+  s.qcap = s.farcap = list_cap(V, rw);
+  s.rowcap = (uint32_t)V;
+  s.outcap = 1 << 16;
+  s.stackcap = 1 << 18;
+  CK(cudaMalloc(&s.table, (size_t)V * rw * 8));
+  CK(cudaMalloc(&s.dist, (size_t)V * DIST_STRIDE * 4));
+  CK(cudaMalloc(&s.rowbits, ((size_t)V + 31) / 32 * 4));
+  for (int i = 0; i < 2; i++) {
+    CK(cudaMalloc(&s.q[i], (size_t)s.qcap * 16));
+    CK(cudaMalloc(&s.far[i], (size_t)s.farcap * 16));
+  }
+  CK(cudaMalloc(&s.rows, (size_t)V * 4));
+  CK(cudaMalloc(&s.out, (size_t)s.outcap * 12));
+  CK(cudaMalloc(&s.stack, (size_t)s.stackcap * 8));
+  CK(cudaMemsetAsync(s.rowbits, 0, ((size_t)V + 31) / 32 * 4, eng->stream));
+  s.bytes = slot_bytes(V, rw);
+  return GST_OK;
+}
+
+size_t row_width(int k, int D) { return ((size_t)1 << k) * (size_t)(D >= 0 ? D + 1 : 1); }
+
+gst_status validate_query(gst_engine* eng, gst_groups* grp, const gst_query* q) {
+  if (!q || q->k < 1 || q->k > KMAX || !q->group_ids)
+    return fail(eng, GST_BAD_INPUT, "query: k must be in [1,8] with group ids");
+  if (q->hop_bound > 30) return fail(eng, GST_BAD_INPUT, "query: hop bound must be <= 30");
+  for (int i = 0; i < q->k; i++) {
+    const int32_t a = q->group_ids[i];
+    if (a < 0 || a >= grp->n) return fail(eng, GST_BAD_INPUT, "query: group id out of range");
+    if (grp->h_ptr[a + 1] == grp->h_ptr[a])
+      return fail(eng, GST_BAD_INPUT, "query: group has no members");
+    for (int j = 0; j < i; j++)
+      if (q->group_ids[j] == a) return fail(eng, GST_BAD_INPUT, "query: duplicate group id");
+  }
+  return GST_OK;
+}
+
+// Host copy of a fresh context for query q in slot s.
+void prep_ctx(gst_engine* eng, gst_graph* g, Slot& s, const gst_query* q, Ctx& c) {
+  memset(&c, 0, sizeof(c));
+  const int hop = q->hop_bound >= 0;
+  c.table = s.table;
+  c.dist = s.dist;
+  c.rowbits = s.rowbits;
+  c.q[0] = s.q[0];
+  c.q[1] = s.q[1];
+  c.far[0] = s.far[0];
+  c.far[1] = s.far[1];
+  c.rows = s.rows;
+  c.out = s.out;
+  c.stack = s.stack;
+  c.qcap = s.qcap;
+  c.farcap = s.farcap;
+  c.rowcap = s.rowcap;
+  c.outcap = s.outcap;
+  c.stackcap = s.stackcap;
+  c.k = q->k;
+  c.W = 1 << q->k;
+  c.full = c.W - 1;
+  c.D = hop ? q->hop_bound : 0;
+  c.DD = hop ? q->hop_bound + 1 : 1;
+  c.RW = c.W * c.DD;
+  c.hop = hop;
+  c.use_lb = hop ? 0 : 1;
+  for (int i = 0; i < q->k; i++) c.gid[i] = q->group_ids[i];
+  c.delta = (uint32_t)std::max(0, eng->cfg.bucket_delta);
+  c.max_levels = (uint32_t)eng->cfg.max_levels;
+  c.in_ptr = nullptr;
+  c.in_n = 0;
+  c.in_kind = 0;
+  c.in_idx = 1;
+  c.no = 0;
+  c.f = 0;
+  c.far_min = 0xFFFFFFFFu;
+  c.bucket_end = c.delta ? c.delta : 0xFFFFFFFFu;
+  c.ub = 0xFFFFFFFFu;
+  c.ub_cell = 0xFFFFFFFFu;
+  c.best = ~0ull;
+  c.phase = c.use_lb ? PH_SSSP : PH_DP;
+}
+
+// Clear the slot's slab and distances for a query with row width rw.
+gst_status reset_slot(gst_engine* eng, gst_graph* g, Slot& s, size_t rw, bool need_dist) {
+  CK(cudaMemsetAsync(s.table, 0xFF, (size_t)g->V * rw * 8, eng->stream));
+  CK(cudaMemsetAsync(s.rowbits, 0, ((size_t)g->V + 31) / 32 * 4, eng->stream));
+  if (need_dist) CK(cudaMemsetAsync(s.dist, 0xFF, (size_t)g->V * DIST_STRIDE * 4, eng->stream));
+  return GST_OK;
+}
+
+struct LoopShape {
+  bool sssp = true;
+  int rw_max = 1;
+};
+
+gst_status launch_level(gst_engine* eng, gst_graph* g, int nctx, const LoopShape& sh) {
+  cudaStream_t st = eng->stream;
+  DevGraph G{g->V, g->E, g->d_beg, g->d_edges};
+  const int split = eng->cfg.split_degree;
+  const int tpb = eng->cfg.threads_per_block;
+  if (sh.sssp) {
+    k_sssp<<<eng->sssp_blocks, 256, 0, st>>>(g->d_ctx, nctx, G, split);
+    k_ctrl<<<1, MAXB, 0, st>>>(g->d_ctx, nctx, CTRL_SSSP);
+  }
+  const size_t per_warp = rows_smem_per_warp(sh.rw_max);
+  const int warps = std::max(1, tpb / 32);
+  k_rows<<<eng->grow_blocks, warps * 32, per_warp * warps, st>>>(g->d_ctx, nctx, G, split,
+                                                                  sh.rw_max);
+  k_ctrl<<<1, MAXB, 0, st>>>(g->d_ctx, nctx, CTRL_DP_ROWS);
+  k_grow<<<eng->grow_blocks, 256, 0, st>>>(g->d_ctx, nctx, G, split);
+  k_ctrl<<<1, MAXB, 0, st>>>(g->d_ctx, nctx, CTRL_DP_GROW);
+  CK(cudaGetLastError());
+  return GST_OK;
+}
+
+gst_status status_of(const Ctx& c) {
+  if (c.error & ERR_TIMEOUT) return GST_TIMEOUT;
+  if (c.error & (ERR_QCAP | ERR_FARCAP | ERR_ROWCAP)) return GST_CAPACITY;
+  if (c.error) return GST_DEVICE_ERROR;
+  if (c.phase != PH_DONE) return GST_DEVICE_ERROR;
+  if (c.best == ~0ull) return GST_INFEASIBLE;
+  return GST_OK;
+}
+
+void fill_result(gst_graph* g, const Ctx& c, const gst_query* q, const std::vector<int32_t>& raw,
+                 gst_result* r) {
+  memset(r, 0, sizeof(*r));
+  r->user_tag = q->user_tag;
+  r->status = status_of(c);
+  r->stats.levels = c.levels;
+  r->stats.states_expanded = (int64_t)c.st_items;
+  r->stats.edge_relaxations = (int64_t)c.st_relax;
+  r->stats.merge_pairs = (int64_t)c.st_merge;
+  r->stats.rows_merged = (int64_t)c.st_rows;
+  r->stats.sssp_relaxations = (int64_t)c.st_sssp;
+  if (r->status != GST_OK) return;
+  r->cost = (int32_t)(c.best >> 32);
+  r->root = (int32_t)(c.best & 0x7FFFFFFull);
+  r->root_hop = (int32_t)((c.best >> 27) & 31u);
+  // distinct edges, (min, max) orientation
+  std::vector<std::pair<std::pair<int32_t, int32_t>, int32_t>> es;
+  const size_t n = std::min<size_t>(c.n_out, raw.size() / 3);
+  es.reserve(n);
+  for (size_t i = 0; i < n; i++) {
+    int32_t a = raw[3 * i], b = raw[3 * i + 1];
+    if (a > b) std::swap(a, b);
+    es.push_back({{a, b}, raw[3 * i + 2]});
+  }
+  std::sort(es.begin(), es.end());
+  es.erase(std::unique(es.begin(), es.end(),
+                       [](const auto& x, const auto& y) { return x.first == y.first; }),
+           es.end());
+  r->n_edges = (int64_t)es.size();
+  if (!es.empty()) {
+    r->edge_u = (int32_t*)malloc(sizeof(int32_t) * es.size());
+    r->edge_v = (int32_t*)malloc(sizeof(int32_t) * es.size());
+    r->edge_w = (int32_t*)malloc(sizeof(int32_t) * es.size());
+    for (size_t i = 0; i < es.size(); i++) {
+      r->edge_u[i] = es[i].first.first;
+      r->edge_v[i] = es[i].first.second;
+      r->edge_w[i] = es[i].second;
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+void gst_config_default(gst_config* cfg) {
+  if (!cfg) return;
+  memset(cfg, 0, sizeof(*cfg));
+  cfg->mem_budget_bytes = 0;
+  cfg->split_degree = 256;
+  cfg->bucket_delta = 0;
+  cfg->max_levels = 1 << 20;
+  cfg->threads_per_block = 256;
+  cfg->blocks_per_sm = 4;
+  cfg->max_batch = 16;
+  cfg->use_graphs = 0;
+  cfg->verbose = 0;
+}
+
+gst_status gst_engine_create(int32_t device, const gst_config* cfg, gst_engine** out) {
+  if (!out) return fail(nullptr, GST_BAD_INPUT, "engine: null output");
+  *out = nullptr;
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0)
+    return fail(nullptr, GST_DEVICE_ERROR, "engine: no CUDA device available");
+  if (device < 0 || device >= ndev) return fail(nullptr, GST_BAD_INPUT, "engine: bad device");
+  gst_engine* eng = new gst_engine();
+  eng->device = device;
+  gst_config_default(&eng->cfg);
+  if (cfg) {
+    gst_config d = eng->cfg;
+    eng->cfg = *cfg;
+    if (eng->cfg.split_degree <= 0) eng->cfg.split_degree = d.split_degree;
+    if (eng->cfg.max_levels <= 0) eng->cfg.max_levels = d.max_levels;
+    if (eng->cfg.threads_per_block <= 0) eng->cfg.threads_per_block = d.threads_per_block;
+    if (eng->cfg.blocks_per_sm <= 0) eng->cfg.blocks_per_sm = d.blocks_per_sm;
+    if (eng->cfg.max_batch <= 0) eng->cfg.max_batch = d.max_batch;
+  }
+  eng->cfg.max_batch = std::min(eng->cfg.max_batch, MAXB);
+  if (cudaSetDevice(device) != cudaSuccess) {
+    delete eng;
+    return fail(nullptr, GST_DEVICE_ERROR, "engine: cudaSetDevice failed");
+  }
+  cudaDeviceProp prop;
+  cudaGetDeviceProperties(&prop, device);
+  eng->sms = prop.multiProcessorCount;
+  eng->grow_blocks = eng->sms * eng->cfg.blocks_per_sm;
+  eng->sssp_blocks = eng->sms * eng->cfg.blocks_per_sm;
+  if (cudaStreamCreateWithFlags(&eng->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&eng->ev0) != cudaSuccess || cudaEventCreate(&eng->ev1) != cudaSuccess) {
+    delete eng;
+    return fail(nullptr, GST_DEVICE_ERROR, "engine: stream/event creation failed");
+  }
+  cudaFuncSetAttribute(k_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  *out = eng;
+  return GST_OK;
+}
+
+gst_status gst_engine_destroy(gst_engine* eng) {
+  if (!eng) return GST_OK;
+  cudaSetDevice(eng->device);
+  if (eng->stream) cudaStreamDestroy(eng->stream);
+  if (eng->ev0) cudaEventDestroy(eng->ev0);
+  if (eng->ev1) cudaEventDestroy(eng->ev1);
+  delete eng;
+  return GST_OK;
+}
+
+const char* gst_last_error_string(gst_engine* eng) {
+  if (eng) {
+    tl_err = eng->err;
+    return tl_err.c_str();
+  }
+  return tl_err.c_str();
+}
+
+static gst_status graph_create_impl(gst_engine* eng, int64_t V, int64_t E, const int64_t* beg,
+                                    const int32_t* adj, const int32_t* wt, gst_graph** out) {
+  if (!eng || !out) return fail(eng, GST_BAD_INPUT, "graph: null argument");
+  *out = nullptr;
+  if (V < 1 || V >= (int64_t)1 << 27 || E < 0 || !beg || (E > 0 && (!adj || !wt)))
+    return fail(eng, GST_BAD_INPUT, "graph: need 1 <= V < 2^27, E >= 0 and non-null arrays");
+  if (beg[0] != 0 || beg[V] != E) return fail(eng, GST_BAD_INPUT, "graph: beg_pos[0] must be 0 and beg_pos[V] == E");
+  std::vector<int2> edges((size_t)E);
+  for (int64_t v = 0; v < V; v++) {
+    if (beg[v + 1] < beg[v]) return fail(eng, GST_BAD_INPUT, "graph: beg_pos not monotone");
+    std::vector<std::pair<int32_t, int32_t>> tmp;
+    tmp.reserve((size_t)(beg[v + 1] - beg[v]));
+    for (int64_t i = beg[v]; i < beg[v + 1]; i++) {
+      if (adj[i] < 0 || adj[i] >= V) return fail(eng, GST_BAD_INPUT, "graph: neighbour id out of range");
+      if (wt[i] < 1 || wt[i] > (1 << 24))
+        return fail(eng, GST_BAD_INPUT, "graph: weights must be in [1, 2^24]");
+      tmp.push_back({adj[i], wt[i]});
+    }
+    if (!std::is_sorted(tmp.begin(), tmp.end())) std::sort(tmp.begin(), tmp.end());
+    for (size_t j = 0; j < tmp.size(); j++) edges[beg[v] + j] = make_int2(tmp[j].first, tmp[j].second);
+  }
+  std::lock_guard<std::mutex> lk(eng->mu);
+  CK(cudaSetDevice(eng->device));
+  gst_graph* g = new gst_graph();
+  g->eng = eng;
+  g->V = V;
+  g->E = E;
+  g->h_beg.assign(beg, beg + V + 1);
+  CK(cudaMalloc(&g->d_beg, sizeof(int64_t) * (V + 1)));
+  CK(cudaMalloc(&g->d_edges, sizeof(int2) * std::max<int64_t>(E, 1)));
+  CK(cudaMalloc(&g->d_ctx, sizeof(Ctx) * MAXB));
+  CK(cudaMallocHost(&g->h_ctx, sizeof(Ctx) * MAXB));
+  // stream-ordered copies, completed before returning: the level kernels run on a
+  // non-blocking stream that does not wait for the legacy default stream
+  CK(cudaMemcpyAsync(g->d_beg, beg, sizeof(int64_t) * (V + 1), cudaMemcpyHostToDevice,
+                     eng->stream));
+  if (E)
+    CK(cudaMemcpyAsync(g->d_edges, edges.data(), sizeof(int2) * E, cudaMemcpyHostToDevice,
+                       eng->stream));
+  CK(cudaStreamSynchronize(eng->stream));
+  *out = g;
+  return GST_OK;
+}
+
+gst_status gst_graph_create(gst_engine* eng, int64_t V, int64_t E, const int64_t* beg_pos,
+                            const int32_t* csr, const int32_t* weight, gst_graph** out) {
+  return graph_create_impl(eng, V, E, beg_pos, csr, weight, out);
+}
+
+gst_status gst_graph_create_i64(gst_engine* eng, int64_t V, int64_t E, const int64_t* beg_pos,
+                                const int64_t* csr, const int64_t* weight, gst_graph** out) {
+  if (E < 0 || (E > 0 && (!csr || !weight))) return fail(eng, GST_BAD_INPUT, "graph: bad arrays");
+  std::vector<int32_t> a((size_t)E), w((size_t)E);
+  for (int64_t i = 0; i < E; i++) {
+    if (csr[i] < 0 || csr[i] >= V) return fail(eng, GST_BAD_INPUT, "graph: neighbour id out of range");
+    if (weight[i] < 1 || weight[i] > (1 << 24))
+      return fail(eng, GST_BAD_INPUT, "graph: weights must be in [1, 2^24]");
+    a[i] = (int32_t)csr[i];
+    w[i] = (int32_t)weight[i];
+  }
+  return graph_create_impl(eng, V, E, beg_pos, a.data(), w.data(), out);
+}
+
+gst_status gst_graph_destroy(gst_graph* g) {
+  if (!g) return GST_OK;
+  gst_engine* eng = g->eng;
+  std::lock_guard<std::mutex> lk(eng->mu);
+  cudaSetDevice(eng->device);
+  cudaStreamSynchronize(eng->stream);
+  for (auto& s : g->slots) free_slot(s);
+  cudaFree(g->d_beg);
+  cudaFree(g->d_edges);
+  cudaFree(g->d_ctx);
+  cudaFreeHost(g->h_ctx);
+  delete g;
+  return GST_OK;
+}
+
+gst_status gst_groups_create(gst_graph* g, int32_t n_groups, const int64_t* grp_ptr,
+                             const int32_t* members, gst_groups** out) {
+  gst_engine* eng = g ? g->eng : nullptr;
+  if (!g || !out || n_groups < 1 || !grp_ptr) return fail(eng, GST_BAD_INPUT, "groups: bad arguments");
+  *out = nullptr;
+  if (grp_ptr[0] != 0) return fail(eng, GST_BAD_INPUT, "groups: grp_ptr[0] must be 0");
+  for (int32_t i = 0; i < n_groups; i++)
+    if (grp_ptr[i + 1] < grp_ptr[i]) return fail(eng, GST_BAD_INPUT, "groups: grp_ptr not monotone");
+  const int64_t M = grp_ptr[n_groups];
+  if (M > 0 && !members) return fail(eng, GST_BAD_INPUT, "groups: null members");
+  for (int64_t j = 0; j < M; j++)
+    if (members[j] < 0 || members[j] >= g->V) return fail(eng, GST_BAD_INPUT, "groups: member out of range");
+  std::lock_guard<std::mutex> lk(eng->mu);
+  CK(cudaSetDevice(eng->device));
+  gst_groups* gr = new gst_groups();
+  gr->g = g;
+  gr->n = n_groups;
+  gr->h_ptr.assign(grp_ptr, grp_ptr + n_groups + 1);
+  CK(cudaMalloc(&gr->d_ptr, sizeof(int64_t) * (n_groups + 1)));
+  CK(cudaMalloc(&gr->d_mem, sizeof(int32_t) * std::max<int64_t>(M, 1)));
+  CK(cudaMemcpyAsync(gr->d_ptr, grp_ptr, sizeof(int64_t) * (n_groups + 1),
+                     cudaMemcpyHostToDevice, eng->stream));
+  if (M)
+    CK(cudaMemcpyAsync(gr->d_mem, members, sizeof(int32_t) * M, cudaMemcpyHostToDevice,
+                       eng->stream));
+  CK(cudaStreamSynchronize(eng->stream));
+  *out = gr;
+  return GST_OK;
+}
+
+gst_status gst_groups_destroy(gst_groups* gr) {
+  if (!gr) return GST_OK;
+  cudaSetDevice(gr->g->eng->device);
+  cudaFree(gr->d_ptr);
+  cudaFree(gr->d_mem);
+  delete gr;
+  return GST_OK;
+}
+
+gst_status gst_solve_batch(gst_graph* g, gst_groups* grp, int32_t n, const gst_query* queries,
+                           gst_result* results) {
+  gst_engine* eng = g ? g->eng : nullptr;
+  if (!g || !grp || grp->g != g || n < 0 || (n > 0 && (!queries || !results)))
+    return fail(eng, GST_BAD_INPUT, "solve: bad arguments");
+  for (int32_t i = 0; i < n; i++) memset(&results[i], 0, sizeof(gst_result));
+  std::lock_guard<std::mutex> lk(eng->mu);
+  CK(cudaSetDevice(eng->device));
+  const int B = std::max(1, std::min<int>(eng->cfg.max_batch, n));
+  // admission: slots sized for the widest query, bounded by the memory budget
+  size_t rw_max = 1;
+  for (int32_t i = 0; i < n; i++) {
+    gst_status s = validate_query(eng, grp, &queries[i]);
+    if (s != GST_OK) {
+      results[i].status = s;
+      results[i].user_tag = queries[i].user_tag;
+      continue;
+    }
+    rw_max = std::max(rw_max, row_width(queries[i].k, queries[i].hop_bound));
+  }
+  size_t free_b = 0, total_b = 0;
+  CK(cudaMemGetInfo(&free_b, &total_b));
+  size_t held = 0;
+  for (auto& s : g->slots) held += s.bytes;
+  const size_t budget = eng->cfg.mem_budget_bytes > 0 ? (size_t)eng->cfg.mem_budget_bytes
+                                                      : (size_t)((free_b + held) * 0.85);
+  const size_t per = slot_bytes(g->V, rw_max);
+  int nslots = (int)std::min<size_t>((size_t)B, budget / std::max<size_t>(per, 1));
+  if (nslots < 1) {
+    for (int32_t i = 0; i < n; i++)
+      if (results[i].status == 0) {
+        results[i].status = GST_OOM_ADMISSION;
+        results[i].user_tag = queries[i].user_tag;
+      }
+    return fail(eng, GST_OOM_ADMISSION, "solve: state table does not fit the memory budget");
+  }
+  for (int s = 0; s < nslots; s++) {
+    gst_status st = ensure_slot(eng, g, (size_t)s, rw_max);
+    if (st != GST_OK) return st;
+  }
+  // slot -> query index; -1 = free
+  std::vector<int> owner(nslots, -1);
+  std::vector<int32_t> raw((size_t)(1 << 16) * 3);
+  int32_t next = 0;
+  auto next_valid = [&]() {
+    while (next < n && results[next].status != 0) next++;
+    return next < n ? next++ : -1;
+  };
+  CK(cudaEventRecord(eng->ev0, eng->stream));
+  int active = 0;
+  // fill and run in waves of refills: a finished slot is refilled at the next check
+  for (;;) {
+    for (int s = 0; s < nslots; s++) {
+      if (owner[s] >= 0) continue;
+      int qi = next_valid();
+      if (qi < 0) break;
+      const gst_query* q = &queries[qi];
+      Slot& sl = g->slots[s];
+      Ctx& hc = g->h_ctx[s];
+      prep_ctx(eng, g, sl, q, hc);
+      gst_status st = reset_slot(eng, g, sl, (size_t)hc.RW, hc.use_lb != 0);
+      if (st != GST_OK) return st;
+      CK(cudaMemcpyAsync(g->d_ctx + s, &hc, sizeof(Ctx), cudaMemcpyHostToDevice, eng->stream));
+      // k_init for this slot alone: grid.y selects the context
+      DevGraph G{g->V, g->E, g->d_beg, g->d_edges};
+      k_init<<<dim3(64, 1), 256, 0, eng->stream>>>(g->d_ctx + s, 1, G, grp->d_ptr, grp->d_mem,
+                                                   eng->cfg.split_degree);
+      k_ctrl<<<1, 32, 0, eng->stream>>>(g->d_ctx + s, 1, CTRL_SSSP);
+      owner[s] = qi;
+      active++;
+    }
+    if (active == 0) break;
+    // contexts of free slots must look finished to the level kernels
+    for (int s = 0; s < nslots; s++)
+      if (owner[s] < 0) {
+        Ctx& idle = g->h_ctx[s];
+        memset(&idle, 0, sizeof(idle));
+        idle.phase = PH_DONE;
+        idle.best = ~0ull;
+        CK(cudaMemcpyAsync(g->d_ctx + s, &idle, sizeof(Ctx), cudaMemcpyHostToDevice, eng->stream));
+      }
+    LoopShape sh;
+    sh.sssp = true;
+    sh.rw_max = (int)rw_max;
+    // run until at least one query finishes
+    const int ahead = 6;
+    bool any_done = false;
+    while (!any_done) {
+      for (int i = 0; i < ahead; i++) {
+        gst_status st = launch_level(eng, g, nslots, sh);
+        if (st != GST_OK) return st;
+      }
+      CK(cudaMemcpyAsync(g->h_ctx, g->d_ctx, sizeof(Ctx) * nslots, cudaMemcpyDeviceToHost,
+                         eng->stream));
+      CK(cudaStreamSynchronize(eng->stream));
+      bool any_sssp = false;
+      for (int s = 0; s < nslots; s++) {
+        if (owner[s] < 0) continue;
+        any_sssp |= g->h_ctx[s].phase == PH_SSSP;
+        any_done |= g->h_ctx[s].phase >= PH_DONE;
+      }
+      sh.sssp = any_sssp;
+    }
+    // harvest finished queries
+    DevGraph G{g->V, g->E, g->d_beg, g->d_edges};
+    k_extract<<<1, MAXB, 0, eng->stream>>>(g->d_ctx, nslots, G);
+    CK(cudaMemcpyAsync(g->h_ctx, g->d_ctx, sizeof(Ctx) * nslots, cudaMemcpyDeviceToHost,
+                       eng->stream));
+    CK(cudaStreamSynchronize(eng->stream));
+    for (int s = 0; s < nslots; s++) {
+      if (owner[s] < 0 || g->h_ctx[s].phase < PH_DONE) continue;
+      const Ctx c = g->h_ctx[s];
+      const uint32_t nout = std::min(c.n_out, g->slots[s].outcap);
+      if (nout) {
+        CK(cudaMemcpyAsync(raw.data(), g->slots[s].out, (size_t)nout * 12,
+                           cudaMemcpyDeviceToHost, eng->stream));
+        CK(cudaStreamSynchronize(eng->stream));
+      }
+      fill_result(g, c, &queries[owner[s]], raw, &results[owner[s]]);
+      if (c.error || c.phase != PH_DONE) {
+        char msg[160];
+        snprintf(msg, sizeof msg, "query %d: phase %u error bits 0x%x bounds site %u levels %u",
+                 owner[s], c.phase, c.error, c.bad_site, c.levels);
+        fail(eng, (gst_status)results[owner[s]].status, msg);
+      }
+      if (c.error & ERR_EXTRACT) results[owner[s]].status = GST_CAPACITY;
+      owner[s] = -1;
+      active--;
+    }
+  }
+  CK(cudaEventRecord(eng->ev1, eng->stream));
+  CK(cudaEventSynchronize(eng->ev1));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, eng->ev0, eng->ev1);
+  for (int32_t i = 0; i < n; i++) results[i].stats.device_ms = ms;
+  return GST_OK;
+}
+
+gst_status gst_solve(gst_graph* g, gst_groups* grp, const gst_query* q, gst_result* res) {
+  gst_engine* eng = g ? g->eng : nullptr;
+  if (!g || !grp || !q || !res) return fail(eng, GST_BAD_INPUT, "solve: null argument");
+  gst_status s = validate_query(eng, grp, q);
+  if (s != GST_OK) {
+    memset(res, 0, sizeof(*res));
+    res->status = s;
+    res->user_tag = q->user_tag;
+    return s;
+  }
+  const int32_t saved = eng->cfg.max_batch;
+  eng->cfg.max_batch = 1;
+  s = gst_solve_batch(g, grp, 1, q, res);
+  eng->cfg.max_batch = saved;
+  if (s != GST_OK) return s;
+  return (gst_status)res->status;
+}
+
+gst_status gst_debug_slot_state(gst_graph* g, int32_t slot, uint64_t* cells, int64_t n_cells,
+                                uint64_t* best_out) {
+  gst_engine* eng = g ? g->eng : nullptr;
+  if (!g || slot < 0 || (size_t)slot >= g->slots.size() || n_cells < 0)
+    return fail(eng, GST_BAD_INPUT, "debug: bad slot");
+  std::lock_guard<std::mutex> lk(eng->mu);
+  CK(cudaSetDevice(eng->device));
+  const Slot& s = g->slots[slot];
+  const int64_t have = (int64_t)(s.V * s.rw_cap);
+  if (cells && n_cells)
+    CK(cudaMemcpyAsync(cells, s.table, (size_t)std::min(n_cells, have) * 8,
+                       cudaMemcpyDeviceToHost, eng->stream));
+  CK(cudaMemcpyAsync(g->h_ctx + slot, g->d_ctx + slot, sizeof(Ctx), cudaMemcpyDeviceToHost,
+                     eng->stream));
+  CK(cudaStreamSynchronize(eng->stream));
+  if (best_out) *best_out = g->h_ctx[slot].best;
+  return GST_OK;
+}
+
+void gst_result_free(gst_result* r) {
+  if (!r) return;
+  free(r->edge_u);
+  free(r->edge_v);
+  free(r->edge_w);
+  r->edge_u = r->edge_v = r->edge_w = nullptr;
+  r->n_edges = 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,140 @@
+/*
+ * gst.h — C ABI of the B200 group Steiner tree (GST) engine.
+ *
+ * One engine is bound to one CUDA device.  A graph is uploaded once and stays
+ * resident in HBM; vertex groups are registered against it; queries name k
+ * groups (and optionally a hop / diameter bound D) and return the optimal tree
+ * cost and the tree's edge set.  Every entry point returns a gst_status; no entry
+ * point exits the process or falls back to a CPU solver.
+ *
+ * What each entry point replaces in the reference (rucdatascience/GPU4GST-sigmod-fullEXP),
+ * whose only interface is a per-experiment executable:
+ *   gst_graph_create      graph<> ctor + gpu_graph upload: code/TrimCDP-WB/include/graph.hpp:12-126,
+ *                         code/TrimCDP-WB/include/gpu_graph.cuh:35-90 (int64 files narrowed to int32)
+ *   gst_graph_create_i64  the same, taking the int64 _beg_pos/_csr/_weight.bin arrays as read
+ *                         (code/TrimCDP-WB/include/graph.hpp:25-112)
+ *   gst_groups_create     read_Group: code/TrimCDP-WB/include/read_group.hpp:9-54
+ *                         (group id in a query = .g id - 1)
+ *   gst_solve (D < 0)     per-query body of code/TrimCDP-WB/src/GSTnonHop.cu:247-497
+ *                         (set_max_ID init, one-label SSSP, lb tables, balanced_push, min over V)
+ *   gst_solve (D >= 0)    per-query body of code/D-TrimCDP-WB/src/GPUHop.cu:172-266 with the
+ *                         answer semantics of code/D-PrunedDP++/include/CPUHOP.h:146-225
+ *                         (minimum over every d <= D)
+ *   gst_solve_batch       the q_start..q_end loop of the same drivers (GSTnonHop.cu:247,
+ *                         GPUHop.cu:172), run as one batched device loop
+ *   result edge set       code/PrunedDP++/include/CPUNONHOP.h:387-429 (build_tree) and
+ *                         code/D-PrunedDP++/include/CPUHOP.h:231-257 — the reference GPU
+ *                         engines return the cost only
+ *   gst_status codes      exit()/assert paths of code/TrimCDP-WB/include/util.h:5-16 and
+ *                         read_group.hpp:47-52; INFEASIBLE replaces the 100000 sentinel
+ *                         (code/TrimCDP-WB/include/header.h:13)
+ */
+#ifndef GST_H
+#define GST_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum gst_status {
+  GST_OK = 0,
+  GST_INFEASIBLE = 1,     /* the queried groups cannot be connected (reference: cost 100000) */
+  GST_OOM_ADMISSION = 2,  /* the query's state table does not fit the device memory budget */
+  GST_BAD_INPUT = 3,      /* malformed graph, groups or query */
+  GST_TIMEOUT = 4,        /* the query exceeded its level budget */
+  GST_DEVICE_ERROR = 5,   /* a CUDA call failed or a kernel reported an error */
+  GST_CAPACITY = 6,       /* a device worklist overflowed its capacity */
+  GST_NOT_READY = 7       /* serving: the polled query has not finished */
+} gst_status;
+
+typedef struct gst_engine gst_engine;
+typedef struct gst_graph gst_graph;
+typedef struct gst_groups gst_groups;
+
+/* Engine tunables; zero fields take defaults (gst_config_default). */
+typedef struct gst_config {
+  int64_t mem_budget_bytes;   /* HBM the engine may use for query state; 0 = 85% of free */
+  int32_t split_degree;       /* edges per grow work item: hubs split into chunks of this size */
+  int32_t bucket_delta;       /* cost-bucket width of the frontier ordering; 0 = autotune */
+  int32_t max_levels;         /* per-query level budget (GST_TIMEOUT beyond) */
+  int32_t threads_per_block;  /* CTA size of the level kernels */
+  int32_t blocks_per_sm;      /* resident CTAs per SM for the level kernels */
+  int32_t max_batch;          /* queries resident at once in gst_solve_batch / serving */
+  int32_t use_graphs;         /* 1: run the level loop as a CUDA graph with a device-side while node */
+  int32_t verbose;
+} gst_config;
+
+typedef struct gst_query {
+  int32_t k;                /* number of groups, 1..8 */
+  const int32_t* group_ids; /* k distinct group ids (0-based, as in <name><k>.csv) */
+  int32_t hop_bound;        /* D >= 0: diameter-bounded query; < 0: no bound */
+  uint64_t user_tag;        /* returned unchanged in the result */
+} gst_query;
+
+typedef struct gst_stats {
+  int64_t levels;           /* DP levels (grow+merge rounds), all phases */
+  int64_t states_expanded;  /* grow work items processed (state x edge chunk) */
+  int64_t edge_relaxations; /* grow relaxations attempted */
+  int64_t merge_pairs;      /* merge pairs evaluated */
+  int64_t rows_merged;      /* vertex rows run through the merge closure */
+  int64_t sssp_relaxations; /* one-label distance relaxations */
+  double device_ms;         /* device time of the query (batch: of the whole batch) */
+} gst_stats;
+
+typedef struct gst_result {
+  int32_t status;     /* gst_status of this query */
+  int32_t cost;       /* optimal cost (valid when status == GST_OK) */
+  int32_t root;       /* root vertex of the DP state holding the optimum */
+  int32_t root_hop;   /* hop index of that state (0 for unbounded queries) */
+  int64_t n_edges;    /* tree edges (duplicates removed) */
+  int32_t* edge_u;    /* engine-allocated, released by gst_result_free */
+  int32_t* edge_v;
+  int32_t* edge_w;
+  uint64_t user_tag;
+  gst_stats stats;
+} gst_result;
+
+void gst_config_default(gst_config* cfg);
+
+gst_status gst_engine_create(int32_t device, const gst_config* cfg, gst_engine** out);
+gst_status gst_engine_destroy(gst_engine* eng);
+/* Message of the last failure on this engine (thread-local copy; never NULL). */
+const char* gst_last_error_string(gst_engine* eng);
+
+/* Graph in CSR with both directions stored (beg_pos[V+1], csr[E], weight[E]);
+ * weights must be >= 1.  The caller keeps ownership of its arrays; the engine
+ * copies them to the device (adjacency sorted per vertex). */
+gst_status gst_graph_create(gst_engine* eng, int64_t V, int64_t E, const int64_t* beg_pos,
+                            const int32_t* csr, const int32_t* weight, gst_graph** out);
+gst_status gst_graph_create_i64(gst_engine* eng, int64_t V, int64_t E, const int64_t* beg_pos,
+                                const int64_t* csr, const int64_t* weight, gst_graph** out);
+gst_status gst_graph_destroy(gst_graph* g);
+
+/* Groups: members of group g are members[grp_ptr[g] .. grp_ptr[g+1]). */
+gst_status gst_groups_create(gst_graph* g, int32_t n_groups, const int64_t* grp_ptr,
+                             const int32_t* members, gst_groups** out);
+gst_status gst_groups_destroy(gst_groups* grp);
+
+/* One query, synchronous.  Fills *res (call gst_result_free afterwards). */
+gst_status gst_solve(gst_graph* g, gst_groups* grp, const gst_query* q, gst_result* res);
+
+/* n queries, run as one batched device loop with up to cfg.max_batch resident at
+ * once; results[i] belongs to queries[i].  Returns GST_OK when every query got a
+ * status (per-query statuses are in the results). */
+gst_status gst_solve_batch(gst_graph* g, gst_groups* grp, int32_t n, const gst_query* queries,
+                           gst_result* results);
+
+void gst_result_free(gst_result* res);
+
+/* Diagnostics (no counterpart in the reference): copy the first n_cells packed
+ * state cells (cost<<32 | pending<<31 | parent) of a query slot and the packed
+ * best full-set state (cost<<32 | hop<<27 | vertex) of the query last run in it. */
+gst_status gst_debug_slot_state(gst_graph* g, int32_t slot, uint64_t* cells, int64_t n_cells,
+                                uint64_t* best_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GST_H */

@@ -1,0 +1,414 @@
+/*
+ * gst_oracle.c — CPU restatement of the reference's exact GST dynamic program.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker for the CUDA engine: only
+ * tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg may load it.
+ * The engine never calls it and has no CPU fallback.
+ *
+ * What it restates (rucdatascience/GPU4GST-sigmod-fullEXP):
+ *   oracle_sssp_groups  multi-source Dijkstra from a vertex group, as
+ *                       graph_v_of_v_idealID_PrunedDPPlusPlus_find_SPs_to_g
+ *                       (code/PrunedDP++/include/CPUNONHOP.h:21-67): a dummy
+ *                       source joined to every member by a 0-weight edge.
+ *   oracle_gst_nonhop   the best-first DPBF recurrence that PrunedDP++ prunes
+ *                       (code/PrunedDP++/include/CPUNONHOP.h:496-957): states
+ *                       (v,p), T(v,p)=0 for every non-empty p inside v's group
+ *                       mask (:593-621), grow along each edge (:797-866), merge
+ *                       T(v,p1)+T(v,p2) with already-popped disjoint p2
+ *                       (:870-955), stop at the first popped full-set state
+ *                       (:655-675); tree rebuilt by the parent walk of
+ *                       graph_v_of_v_idealID_PrunedDPPlusPlus_build_tree
+ *                       (:387-429).  The cost is the same optimum PrunedDP++
+ *                       returns (its pruning only skips states that cannot be on
+ *                       an optimal tree); the returned tree may differ on ties.
+ *   oracle_gst_hop      HOP_cpu (code/D-PrunedDP++/include/CPUHOP.h:107-283):
+ *                       states (v,p,d), singletons (v,{i},0) (:153-168), grow to
+ *                       d+1 while d<D (:190-204), merge with any current
+ *                       (v,p2,d2), d2<=D-d, into max(d,d2) (:205-225), stop at
+ *                       the first popped full-set state at any d<=D (:184-188),
+ *                       parent walk (:231-257).
+ *
+ * Parity pin: tests/golden/ holds costs produced by the reference's own CPU
+ * solvers (compiled unmodified under oracle/_ref by oracle/Makefile) on seeded
+ * inputs; tests check this file against them.
+ *
+ * Costs are int64 here; "infeasible" is reported as -1 (the reference prints its
+ * sentinel 100000, code/PrunedDP++/include/exp_CPU_nonHop.h:120-126).
+ */
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define ORACLE_INF ((int64_t)1 << 60)
+
+/* ---- binary min-heap of (key, a, b, c) with lazy deletion ----------------- */
+typedef struct {
+  int64_t key;
+  int32_t v;
+  int32_t p;
+  int32_t d;
+} hitem;
+
+typedef struct {
+  hitem* a;
+  int64_t n, cap;
+} heap_t;
+
+static int hless(const hitem* x, const hitem* y) {
+  if (x->key != y->key) return x->key < y->key;
+  if (x->v != y->v) return x->v < y->v;
+  if (x->p != y->p) return x->p < y->p;
+  return x->d < y->d;
+}
+
+static int heap_push(heap_t* h, hitem it) {
+  if (h->n == h->cap) {
+    int64_t nc = h->cap ? h->cap * 2 : 1024;
+    hitem* na = (hitem*)realloc(h->a, sizeof(hitem) * nc);
+    if (!na) return -1;
+    h->a = na;
+    h->cap = nc;
+  }
+  int64_t i = h->n++;
+  h->a[i] = it;
+  while (i > 0) {
+    int64_t p = (i - 1) / 2;
+    if (!hless(&h->a[i], &h->a[p])) break;
+    hitem t = h->a[i];
+    h->a[i] = h->a[p];
+    h->a[p] = t;
+    i = p;
+  }
+  return 0;
+}
+
+static hitem heap_pop(heap_t* h) {
+  hitem top = h->a[0];
+  h->a[0] = h->a[--h->n];
+  int64_t i = 0;
+  for (;;) {
+    int64_t l = 2 * i + 1, r = l + 1, m = i;
+    if (l < h->n && hless(&h->a[l], &h->a[m])) m = l;
+    if (r < h->n && hless(&h->a[r], &h->a[m])) m = r;
+    if (m == i) break;
+    hitem t = h->a[i];
+    h->a[i] = h->a[m];
+    h->a[m] = t;
+    i = m;
+  }
+  return top;
+}
+
+/* ---- helpers -------------------------------------------------------------- */
+static int32_t edge_weight(const int64_t* beg, const int32_t* adj, const int32_t* w, int32_t a,
+                           int32_t b) {
+  for (int64_t i = beg[a]; i < beg[a + 1]; i++)
+    if (adj[i] == b) return w[i];
+  return -1;
+}
+
+/* group-membership mask of each vertex for the k query groups (bit i = i-th id) */
+static uint32_t* query_masks(int64_t V, const int64_t* grp_ptr, const int32_t* members,
+                             int32_t k, const int32_t* group_ids) {
+  uint32_t* m = (uint32_t*)calloc((size_t)V, sizeof(uint32_t));
+  if (!m) return NULL;
+  for (int32_t i = 0; i < k; i++) {
+    int32_t g = group_ids[i];
+    for (int64_t j = grp_ptr[g]; j < grp_ptr[g + 1]; j++) m[members[j]] |= 1u << i;
+  }
+  return m;
+}
+
+typedef struct {
+  int32_t a, b, w;
+} tedge;
+
+static int cmp_tedge(const void* x, const void* y) {
+  const tedge* p = (const tedge*)x;
+  const tedge* q = (const tedge*)y;
+  if (p->a != q->a) return p->a < q->a ? -1 : 1;
+  if (p->b != q->b) return p->b < q->b ? -1 : 1;
+  return 0;
+}
+
+/* sort + unique the collected edges (the reference collects them in a hash
+ * graph, so duplicates collapse), copy out, return the distinct count */
+static int64_t emit_edges(tedge* e, int64_t n, int64_t cap, int32_t* eu, int32_t* ev,
+                          int32_t* ew, int64_t* wsum) {
+  qsort(e, (size_t)n, sizeof(tedge), cmp_tedge);
+  int64_t m = 0;
+  *wsum = 0;
+  for (int64_t i = 0; i < n; i++) {
+    if (i > 0 && e[i].a == e[i - 1].a && e[i].b == e[i - 1].b) continue;
+    if (m < cap) {
+      eu[m] = e[i].a;
+      ev[m] = e[i].b;
+      ew[m] = e[i].w;
+    }
+    *wsum += e[i].w;
+    m++;
+  }
+  return m;
+}
+
+/* ---- multi-source Dijkstra ------------------------------------------------ */
+int oracle_sssp_groups(int64_t V, const int64_t* beg, const int32_t* adj, const int32_t* w,
+                       int64_t n_src, const int32_t* src, int64_t* dist) {
+  heap_t h = {0};
+  for (int64_t v = 0; v < V; v++) dist[v] = ORACLE_INF;
+  for (int64_t i = 0; i < n_src; i++) {
+    dist[src[i]] = 0;
+    hitem it = {0, src[i], 0, 0};
+    if (heap_push(&h, it)) return 1;
+  }
+  while (h.n) {
+    hitem it = heap_pop(&h);
+    if (it.key != dist[it.v]) continue;
+    for (int64_t e = beg[it.v]; e < beg[it.v + 1]; e++) {
+      int64_t nd = it.key + w[e];
+      if (nd < dist[adj[e]]) {
+        dist[adj[e]] = nd;
+        hitem ni = {nd, adj[e], 0, 0};
+        if (heap_push(&h, ni)) return 1;
+      }
+    }
+  }
+  free(h.a);
+  return 0;
+}
+
+/* ---- non-hop exact DP ----------------------------------------------------- */
+/* Returns 0 on success.  *cost = optimum (-1 if the groups cannot be connected),
+ * *root = vertex of the popped full-set state, *n_edges = distinct tree edges
+ * (written up to edge_cap), *edge_sum = their weight sum, *pops = states popped. */
+int oracle_gst_nonhop(int64_t V, const int64_t* beg, const int32_t* adj, const int32_t* w,
+                      const int64_t* grp_ptr, const int32_t* members, int32_t k,
+                      const int32_t* group_ids, int64_t* cost, int32_t* root, int64_t* n_edges,
+                      int64_t edge_cap, int32_t* eu, int32_t* ev, int32_t* ew, int64_t* edge_sum,
+                      int64_t* pops) {
+  if (k < 1 || k > 16) return 1;
+  const int32_t W = 1 << k, FULL = W - 1;
+  uint32_t* mask = query_masks(V, grp_ptr, members, k, group_ids);
+  int64_t* c = (int64_t*)malloc(sizeof(int64_t) * (size_t)V * W);
+  int32_t* par = (int32_t*)malloc(sizeof(int32_t) * (size_t)V * W); /* grow: -1-u ; merge: p1 */
+  uint8_t* done = (uint8_t*)calloc((size_t)V * W, 1);
+  if (!mask || !c || !par || !done) return 2;
+  for (int64_t i = 0; i < V * W; i++) c[i] = ORACLE_INF;
+  heap_t h = {0};
+  for (int64_t v = 0; v < V; v++) {
+    uint32_t m = mask[v];
+    for (uint32_t p = m; p; p = (p - 1) & m) {
+      c[v * W + p] = 0;
+      par[v * W + p] = 0; /* leaf */
+      hitem it = {0, (int32_t)v, (int32_t)p, 0};
+      heap_push(&h, it);
+    }
+  }
+  int64_t npop = 0;
+  int32_t rv = -1;
+  while (h.n) {
+    hitem it = heap_pop(&h);
+    const int64_t s = (int64_t)it.v * W + it.p;
+    if (done[s] || it.key != c[s]) continue;
+    done[s] = 1;
+    npop++;
+    if (it.p == FULL) {
+      rv = it.v;
+      break;
+    }
+    const int64_t cv = it.key;
+    for (int64_t e = beg[it.v]; e < beg[it.v + 1]; e++) {
+      const int64_t t = (int64_t)adj[e] * W + it.p;
+      if (!done[t] && cv + w[e] < c[t]) {
+        c[t] = cv + w[e];
+        par[t] = -1 - it.v;
+        hitem ni = {c[t], adj[e], it.p, 0};
+        heap_push(&h, ni);
+      }
+    }
+    const uint32_t comp = (uint32_t)FULL & ~(uint32_t)it.p;
+    for (uint32_t q = comp; q; q = (q - 1) & comp) {
+      const int64_t sq = (int64_t)it.v * W + q;
+      if (!done[sq]) continue;
+      const int64_t t = (int64_t)it.v * W + (it.p | q);
+      const int64_t nc = cv + c[sq];
+      if (!done[t] && nc < c[t]) {
+        c[t] = nc;
+        par[t] = it.p; /* p1; p2 = (p|q) ^ p1 */
+        hitem ni = {nc, it.v, (int32_t)(it.p | q), 0};
+        heap_push(&h, ni);
+      }
+    }
+  }
+  *pops = npop;
+  *root = rv;
+  *n_edges = 0;
+  *edge_sum = 0;
+  if (rv < 0) {
+    *cost = -1;
+  } else {
+    *cost = c[(int64_t)rv * W + FULL];
+    /* parent walk: queue of (v,p) */
+    int64_t qcap = 1024, qh = 0, qt = 0, ecap = 1024, ne = 0;
+    int64_t* qs = (int64_t*)malloc(sizeof(int64_t) * qcap);
+    tedge* es = (tedge*)malloc(sizeof(tedge) * ecap);
+    qs[qt++] = (int64_t)rv * W + FULL;
+    while (qh < qt) {
+      const int64_t s = qs[qh++];
+      const int32_t v = (int32_t)(s / W), p = (int32_t)(s % W);
+      int64_t add[2];
+      int na = 0;
+      if (c[s] == 0 && ((uint32_t)p & ~mask[v]) == 0) {
+        /* leaf: v covers p */
+      } else if (par[s] < 0) {
+        const int32_t u = -1 - par[s];
+        if (ne == ecap) es = (tedge*)realloc(es, sizeof(tedge) * (ecap *= 2));
+        es[ne].a = u < v ? u : v;
+        es[ne].b = u < v ? v : u;
+        es[ne].w = edge_weight(beg, adj, w, u, v);
+        ne++;
+        add[na++] = (int64_t)u * W + p;
+      } else {
+        const int32_t p1 = par[s], p2 = p ^ p1;
+        add[na++] = (int64_t)v * W + p1;
+        add[na++] = (int64_t)v * W + p2;
+      }
+      for (int i = 0; i < na; i++) {
+        if (qt == qcap) qs = (int64_t*)realloc(qs, sizeof(int64_t) * (qcap *= 2));
+        qs[qt++] = add[i];
+      }
+    }
+    *n_edges = emit_edges(es, ne, edge_cap, eu, ev, ew, edge_sum);
+    free(qs);
+    free(es);
+  }
+  free(h.a);
+  free(mask);
+  free(c);
+  free(par);
+  free(done);
+  return 0;
+}
+
+/* ---- hop-bounded DP (HOP_cpu) --------------------------------------------- */
+int oracle_gst_hop(int64_t V, const int64_t* beg, const int32_t* adj, const int32_t* w,
+                   const int64_t* grp_ptr, const int32_t* members, int32_t k,
+                   const int32_t* group_ids, int32_t D, int64_t* cost, int32_t* root,
+                   int32_t* root_d, int64_t* n_edges, int64_t edge_cap, int32_t* eu, int32_t* ev,
+                   int32_t* ew, int64_t* edge_sum, int64_t* pops) {
+  if (k < 1 || k > 16 || D < 0 || D > 64) return 1;
+  const int32_t W = 1 << k, FULL = W - 1, DD = D + 1;
+  const int64_t S = V * W * DD;
+  uint32_t* mask = query_masks(V, grp_ptr, members, k, group_ids);
+  int64_t* c = (int64_t*)malloc(sizeof(int64_t) * (size_t)S);
+  /* parent: type(2 bits) | payload: grow -> u ; merge -> p1, d1, d2 */
+  uint8_t* typ = (uint8_t*)calloc((size_t)S, 1);
+  int32_t* pa = (int32_t*)malloc(sizeof(int32_t) * (size_t)S);
+  int32_t* pb = (int32_t*)malloc(sizeof(int32_t) * (size_t)S);
+  if (!mask || !c || !typ || !pa || !pb) return 2;
+  for (int64_t i = 0; i < S; i++) c[i] = ORACLE_INF;
+  heap_t h = {0};
+#define IDX(v, p, d) (((int64_t)(v) * W + (p)) * DD + (d))
+  for (int64_t v = 0; v < V; v++) {
+    for (int32_t i = 0; i < k; i++)
+      if (mask[v] >> i & 1) {
+        c[IDX(v, 1 << i, 0)] = 0;
+        hitem it = {0, (int32_t)v, 1 << i, 0};
+        heap_push(&h, it);
+      }
+  }
+  int64_t npop = 0;
+  int32_t rv = -1, rp = 0, rd = 0;
+  while (h.n) {
+    hitem it = heap_pop(&h);
+    const int32_t v = it.v, p = it.p, d = it.d;
+    const int64_t cv = it.key;
+    if (cv != c[IDX(v, p, d)]) continue;
+    npop++;
+    if (p == FULL) {
+      rv = v;
+      rp = p;
+      rd = d;
+      break;
+    }
+    if (d < D) {
+      for (int64_t e = beg[v]; e < beg[v + 1]; e++) {
+        const int64_t t = IDX(adj[e], p, d + 1);
+        if (c[t] > cv + w[e]) {
+          c[t] = cv + w[e];
+          typ[t] = 1;
+          pa[t] = v;
+          hitem ni = {c[t], adj[e], p, d + 1};
+          heap_push(&h, ni);
+        }
+      }
+    }
+    for (int32_t p2 = 1; p2 <= FULL; p2++) {
+      if (p2 & p) continue;
+      for (int32_t d2 = 0; d2 <= D - d; d2++) {
+        const int64_t c2 = c[IDX(v, p2, d2)];
+        if (c2 >= ORACLE_INF) continue;
+        const int32_t nd = d > d2 ? d : d2;
+        const int64_t t = IDX(v, p | p2, nd);
+        if (c[t] > cv + c2) {
+          c[t] = cv + c2;
+          typ[t] = 2;
+          pa[t] = p;
+          pb[t] = (d << 8) | d2;
+          hitem ni = {c[t], v, p | p2, nd};
+          heap_push(&h, ni);
+        }
+      }
+    }
+  }
+  *pops = npop;
+  *root = rv;
+  *root_d = rd;
+  *n_edges = 0;
+  *edge_sum = 0;
+  if (rv < 0) {
+    *cost = -1;
+  } else {
+    *cost = c[IDX(rv, rp, rd)];
+    int64_t qcap = 1024, qh = 0, qt = 0, ecap = 1024, ne = 0;
+    int64_t* qs = (int64_t*)malloc(sizeof(int64_t) * qcap);
+    tedge* es = (tedge*)malloc(sizeof(tedge) * ecap);
+    qs[qt++] = IDX(rv, rp, rd);
+    while (qh < qt) {
+      const int64_t s = qs[qh++];
+      const int32_t d = (int32_t)(s % DD);
+      const int32_t p = (int32_t)((s / DD) % W);
+      const int32_t v = (int32_t)(s / DD / W);
+      int64_t add[2];
+      int na = 0;
+      if (typ[s] == 1) {
+        const int32_t u = pa[s];
+        if (ne == ecap) es = (tedge*)realloc(es, sizeof(tedge) * (ecap *= 2));
+        es[ne].a = u < v ? u : v;
+        es[ne].b = u < v ? v : u;
+        es[ne].w = edge_weight(beg, adj, w, u, v);
+        ne++;
+        add[na++] = IDX(u, p, d - 1);
+      } else if (typ[s] == 2) {
+        const int32_t p1 = pa[s], d1 = pb[s] >> 8, d2 = pb[s] & 0xff;
+        add[na++] = IDX(v, p1, d1);
+        add[na++] = IDX(v, p ^ p1, d2);
+      }
+      for (int i = 0; i < na; i++) {
+        if (qt == qcap) qs = (int64_t*)realloc(qs, sizeof(int64_t) * (qcap *= 2));
+        qs[qt++] = add[i];
+      }
+    }
+    *n_edges = emit_edges(es, ne, edge_cap, eu, ev, ew, edge_sum);
+    free(qs);
+    free(es);
+  }
+#undef IDX
+  free(h.a);
+  free(mask);
+  free(c);
+  free(typ);
+  free(pa);
+  free(pb);
+  return 0;
+}

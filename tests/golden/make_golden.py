@@ -1,0 +1,135 @@
+"""Generate the golden fixtures in this directory by running the REFERENCE's own
+CPU solvers (PrunedDP++, TrimCDP-multi-core-CPU, D-PrunedDP++ from
+rucdatascience/GPU4GST-sigmod-fullEXP, compiled unmodified by oracle/Makefile into
+oracle/_ref/) on seeded synthetic inputs written in the reference's file formats.
+
+    make -C oracle ref && python tests/golden/make_golden.py
+
+Each fixture records how to regenerate its inputs (generator + seeds), a
+fingerprint of the generated arrays (so generator drift is caught), the queries,
+and the costs the reference printed in its result CSVs (100000 = no solution).
+Only this script and the oracle need /root/reference; the committed JSON is all
+the tests read.
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import sys
+import tempfile
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "gpu4gst-sigmod-fullexp_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+import numpy as np  # noqa: E402
+
+import gst_b200 as G  # noqa: E402
+import oracle as O  # noqa: E402
+
+
+def fingerprint(g, grp) -> str:
+    h = hashlib.sha256()
+    for a in (g.beg_pos, g.adj, g.weight, grp.grp_ptr, grp.members):
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()[:16]
+
+
+def make_inputs(spec):
+    gs = spec["graph"]
+    if gs["kind"] == "ba":
+        g = G.synth_ba(gs["V"], gs["m"], gs["seed"])
+    elif gs["kind"] == "rmat":
+        g = G.synth_rmat(gs["V"], gs["E"], gs["seed"])
+    else:
+        raise ValueError(gs["kind"])
+    gr = spec["groups"]
+    if gr["kind"] == "uniform":
+        grp = G.synth_groups_uniform(g.V, gr["n"], gr["smin"], gr["smax"], gr["seed"])
+    else:
+        grp = G.synth_groups_zipf(g.V, gr["n"], gr["s"], gr["smin"], gr["smax"], gr["seed"])
+    return g, grp
+
+
+SPECS = [
+    {"name": "c1_ba20k_k3",
+     "graph": {"kind": "ba", "V": 20000, "m": 4, "seed": 0x6057 + 1},
+     "groups": {"kind": "uniform", "n": 500, "smin": 5, "smax": 50, "seed": 0x6057 + 1001},
+     "queries": [{"k": 3, "n": 100, "seed": 0x6057 + 2001, "hop": [None]}],
+     "solvers": ["PrunedDP++", "TrimCDP-multi-core-CPU"]},
+    {"name": "rmat3k_k4_k5",
+     "graph": {"kind": "rmat", "V": 3000, "E": 12000, "seed": 77},
+     "groups": {"kind": "zipf", "n": 200, "s": 1.5, "smin": 2, "smax": 100, "seed": 78},
+     "queries": [{"k": 4, "n": 40, "seed": 83, "hop": [None, 2, 3, 4]},
+                 {"k": 5, "n": 40, "seed": 84, "hop": [None, 3, 4]}],
+     "solvers": ["PrunedDP++", "TrimCDP-multi-core-CPU", "D-PrunedDP++"]},
+    {"name": "rmat20k_k6",
+     "graph": {"kind": "rmat", "V": 20000, "E": 150000, "seed": 91},
+     "groups": {"kind": "zipf", "n": 1000, "s": 1.5, "smin": 2, "smax": 200, "seed": 92},
+     "queries": [{"k": 6, "n": 20, "seed": 93, "hop": [None, 3]}],
+     "solvers": ["PrunedDP++", "D-PrunedDP++"]},
+]
+
+
+def run_spec(spec):
+    g, grp = make_inputs(spec)
+    out = {"name": spec["name"], "graph": spec["graph"], "groups": spec["groups"],
+           "V": g.V, "E": g.E, "fingerprint": fingerprint(g, grp), "cases": []}
+    with tempfile.TemporaryDirectory() as d:
+        for qs in spec["queries"]:
+            q = G.synth_queries(grp.n_groups, qs["n"], qs["k"], qs["seed"])
+            G.write_reference_files(d, "fx", g, grp, q)
+            for hop in qs["hop"]:
+                case = {"k": qs["k"], "hop": hop, "query_seed": qs["seed"],
+                        "queries": q.tolist(), "ref": {}}
+                for s in spec["solvers"]:
+                    is_hop = O.REF_SOLVERS[s][1]
+                    if is_hop != (hop is not None):
+                        continue
+                    rows, wall = O.run_ref(s, d, "fx", qs["k"], 0, qs["n"] - 1, hop_bound=hop)
+                    rows.sort(key=lambda r: r["task_id"])
+                    case["ref"][s] = [r["cost"] for r in rows]
+                    print(spec["name"], "k", qs["k"], "hop", hop, s, f"{wall:.1f}s", flush=True)
+                out["cases"].append(case)
+    return out
+
+
+KNOWN_ANSWER = {
+    # hand-checked small instances: edges (u, v, w), groups, queries with costs
+    "name": "known_answer",
+    "graphs": [
+        {"V": 4, "edges": [[0, 1, 3], [1, 2, 4], [2, 3, 5]],
+         "groups": [[0], [3], [1, 2], [0, 3]],
+         "cases": [{"q": [0, 1], "hop": None, "cost": 12},
+                   {"q": [0, 2], "hop": None, "cost": 3},
+                   {"q": [3], "hop": None, "cost": 0},
+                   {"q": [0, 1], "hop": 3, "cost": 12},
+                   {"q": [0, 1], "hop": 2, "cost": -1},
+                   {"q": [0, 1, 2], "hop": None, "cost": 12}]},
+        {"V": 5, "edges": [[0, 1, 2], [0, 2, 2], [0, 3, 2], [1, 4, 1], [4, 3, 1]],
+         "groups": [[1], [2], [3], [4]],
+         "cases": [{"q": [0, 1, 2], "hop": None, "cost": 6},
+                   {"q": [0, 1, 2], "hop": 2, "cost": 6},
+                   {"q": [0, 2], "hop": None, "cost": 2},
+                   {"q": [1, 3], "hop": None, "cost": 5}]},
+        {"V": 6, "edges": [[0, 1, 1], [1, 2, 1], [3, 4, 1], [4, 5, 1]],
+         "groups": [[0], [5], [2, 3]],
+         "cases": [{"q": [0, 1], "hop": None, "cost": -1},
+                   {"q": [0, 2], "hop": None, "cost": 2},
+                   {"q": [2], "hop": 0, "cost": 0}]},
+    ],
+}
+
+
+def main():
+    fixtures = [run_spec(s) for s in SPECS]
+    for f in fixtures:
+        with open(os.path.join(HERE, f["name"] + ".json"), "w") as fh:
+            json.dump(f, fh, separators=(",", ":"))
+    with open(os.path.join(HERE, "known_answer.json"), "w") as fh:
+        json.dump(KNOWN_ANSWER, fh, indent=1)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,67 @@
+"""The oracle (CPU restatement of the reference DP) against the reference's own
+outputs: golden costs printed by PrunedDP++, TrimCDP-multi-core-CPU and
+D-PrunedDP++ on seeded inputs (tests/golden/make_golden.py), and hand-checked
+known answers.  Runs on the CPU."""
+import numpy as np
+import pytest
+
+import gst_b200 as G
+import oracle as O
+from conftest import golden_inputs, known_answer_graphs, load_golden
+
+REF_INF = 100000  # the reference's "no solution" sentinel (header.h:13)
+
+
+def _ref_cost(c):
+    return -1 if c >= REF_INF else c
+
+
+@pytest.mark.parametrize("name", ["c1_ba20k_k3", "rmat3k_k4_k5", "rmat20k_k6"])
+def test_oracle_matches_reference_golden(name):
+    fx = load_golden(name)
+    g, grp = golden_inputs(fx)
+    limit = 10 if name == "rmat20k_k6" else None  # the k=6 DP takes seconds per query here
+    for case in fx["cases"]:
+        qs = case["queries"][:limit]
+        for solver, costs in case["ref"].items():
+            for qi, q in enumerate(qs):
+                if case["hop"] is None:
+                    o = O.gst_nonhop(g, grp, q)
+                else:
+                    o = O.gst_hop(g, grp, q, case["hop"])
+                assert o["cost"] == _ref_cost(costs[qi]), (name, solver, case["hop"], qi)
+
+
+def test_oracle_trees_verify():
+    fx = load_golden("rmat3k_k4_k5")
+    g, grp = golden_inputs(fx)
+    for case in fx["cases"]:
+        hop = case["hop"]
+        for q in case["queries"][:15]:
+            o = O.gst_nonhop(g, grp, q) if hop is None else O.gst_hop(g, grp, q, hop)
+            if o["cost"] < 0:
+                continue
+            assert o["edge_sum"] == o["cost"]
+            rc = G.verify_tree(g, grp, q, -1 if hop is None else hop, o["cost"], o["edges"],
+                               o["root"])
+            assert rc == 0, G.VERIFY_CODES[rc]
+
+
+def test_oracle_known_answers():
+    for g, grp, cases in known_answer_graphs():
+        for c in cases:
+            o = O.gst_nonhop(g, grp, c["q"]) if c["hop"] is None else \
+                O.gst_hop(g, grp, c["q"], c["hop"])
+            assert o["cost"] == c["cost"], c
+
+
+def test_oracle_sssp_matches_dp_singletons():
+    fx = load_golden("rmat3k_k4_k5")
+    g, grp = golden_inputs(fx)
+    # distance from group 3 to its own members is 0 and to neighbours <= edge weight
+    mem = grp.members[grp.grp_ptr[3]:grp.grp_ptr[4]]
+    d = O.sssp_groups(g, mem)
+    assert (d[mem] == 0).all()
+    for v in mem:
+        for e in range(g.beg_pos[v], g.beg_pos[v + 1]):
+            assert d[g.adj[e]] <= g.weight[e]
