@@ -1,0 +1,351 @@
+"""Benchmark: exact-cost GST queries/s on the mid-scale power-law workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload c2|c1] [--batch B]
+
+Workload (default "c2", the reference's plain single-query GPU configuration at
+mid scale): R-MAT (a,b,c) = (0.57, 0.19, 0.19), V = 170,000 target, 6.8M
+undirected edges, largest component kept, int32 weights uniform in [1,100];
+5,000 groups with Zipf(1.5) sizes clamped to [2,500]; 300 queries at k=5 and 300
+at k=7 (uniform distinct group ids).  All inputs are seeded synthetic data
+generated here (the reference's datasets are not distributed with it).
+
+One step = one batch of B queries (alternating k=5 / k=7 from the pool) solved
+exactly by the engine through its C ABI (gst_solve_batch), graph resident in HBM.
+L2 is flushed (a 512 MB write) between timed steps.
+
+value   : queries/s over the K timed steps, device time (CUDA events on the
+          engine's stream bracketing each batch), max over ranks.
+e2e     : the same steps timed on the host around the C-ABI call, which uploads
+          each query from host memory and copies every result (cost + tree
+          edges) back; the bytes moved are counted by the engine.
+roofline: the grow kernel (dominant launch): algorithmic bytes
+          24 B x work items + 16 B x edge relaxations, over its event-timed
+          duration in the timed region, against the measured HBM copy bandwidth.
+cpu_baseline: the reference's own PrunedDP++ (oracle/_ref, 1 thread) on a
+          bounded sample of the same queries.
+--impl reference: the reference's TrimCDP-multi-core-CPU on the host cores, on a
+          bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "gpu4gst-sigmod-fullexp_b200")
+ORACLE = os.path.join(ROOT, "oracle")
+sys.path.insert(0, PKG)
+
+METRIC = "exact-cost GST queries/s, batched vs per-query on 1 B200; p50/p99 latency"
+SEED = 0x6057
+
+WORKLOADS = {
+    "c2": dict(name="rmat170k_6.8M_k5k7", graph=("rmat", 170_000, 6_800_000, SEED + 2),
+               groups=("zipf", 5000, 1.5, 2, 500, SEED + 1002),
+               queries=[(5, 300, SEED + 2002), (7, 300, SEED + 2003)]),
+    "c1": dict(name="ba20k_k3", graph=("ba", 20_000, 4, SEED + 1),
+               groups=("uniform", 500, 5, 50, SEED + 1001),
+               queries=[(3, 100, SEED + 2001)]),
+}
+
+
+def make_workload(key):
+    import gst_b200 as G
+    w = WORKLOADS[key]
+    gk = w["graph"]
+    if gk[0] == "rmat":
+        g = G.synth_rmat(gk[1], gk[2], gk[3])
+    else:
+        g = G.synth_ba(gk[1], gk[2], gk[3])
+    gr = w["groups"]
+    if gr[0] == "zipf":
+        grp = G.synth_groups_zipf(g.V, gr[1], gr[2], gr[3], gr[4], gr[5])
+    else:
+        grp = G.synth_groups_uniform(g.V, gr[1], gr[2], gr[3], gr[4])
+    pools = [G.synth_queries(grp.n_groups, n, k, s) for k, n, s in w["queries"]]
+    # interleave the k classes: k5, k7, k5, k7, ...
+    queries = []
+    for i in range(max(len(p) for p in pools)):
+        for p in pools:
+            if i < len(p):
+                queries.append(p[i])
+    return w, g, grp, queries
+
+
+class Clocks:
+    """nvidia-smi samples (SM clock, throttle reasons) during the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi") is None:
+            return self
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        self.proc = subprocess.Popen(
+            ["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+             "--format=csv,noheader,nounits", "-lms", "200"],
+            stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for n, v in zip(names, s[4:8]):
+                if v.strip().lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.samples)}
+
+
+def peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def dist_env():
+    n = int(os.environ.get("WORLD_SIZE", "1"))
+    r = int(os.environ.get("RANK", "0"))
+    lr = int(os.environ.get("LOCAL_RANK", str(r)))
+    return n, r, lr
+
+
+def cpu_reference_sample(w, g, grp, queries, solver, budget_s, threads_note):
+    """Run one of the reference's CPU solvers (oracle/_ref) on a bounded sample of
+    the workload's queries; returns (queries/s end-to-end, per-query main-loop
+    seconds, n done, sample description)."""
+    sys.path.insert(0, ORACLE)
+    import gst_b200 as G
+    import oracle as O
+    if not O.ref_available(solver):
+        return None
+    d = tempfile.mkdtemp(prefix="gstref_")
+    try:
+        ks = sorted({len(q) for q in queries})
+        done, loop_s, wall_s = 0, 0.0, 0.0
+        per_k = {}
+        for k in ks:
+            qk = [q for q in queries if len(q) == k]
+            import numpy as np
+            G.write_reference_files(d, "w", g, grp, np.asarray(qk, dtype=np.int32))
+            # load-only run (q_start > q_end) to separate graph loading from queries
+            _, load_wall = O.run_ref(solver, d, "w", k, 1, 0)
+            n = 0
+            t_k = 0.0
+            while n < len(qk) and wall_s < budget_s:
+                rows, wall = O.run_ref(solver, d, "w", k, n, n, timeout=max(30.0, budget_s))
+                q_wall = max(wall - load_wall, 1e-9)
+                wall_s += q_wall
+                t_k += q_wall
+                loop_s += sum(r["time"] for r in rows)
+                n += 1
+            per_k[k] = (n, t_k)
+            done += n
+        if done == 0:
+            return None
+        sample = ", ".join(f"{n} k={k} queries" for k, (n, _) in per_k.items())
+        return done / wall_s, loop_s / done, done, sample + threads_note
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
+def run_reference_arm(args):
+    n, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    w, g, grp, queries = make_workload(args.workload)
+    threads = min(os.cpu_count() or 1, 100)
+    budget = 20.0
+    res = cpu_reference_sample(w, g, grp, queries[: max(4, args.batch)],
+                               "TrimCDP-multi-core-CPU", budget,
+                               f"; TrimCDP-multi-core-CPU, {threads} threads")
+    if res is None:
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/TrimCDP-multi-core-CPU not built"}))
+        return 0
+    qps, loop, done, sample = res
+    line = {
+        "metric": METRIC, "value": qps, "unit": "queries/s", "n_gpus": n, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * args.batch / qps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": w["name"], "global_batch": args.batch, "parallelism": "cpu"},
+        "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": threads,
+                         "kind": "reference", "sample": sample},
+        "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args):
+    import numpy as np
+    import gst_b200 as G
+    n_ranks, rank, local_rank = dist_env()
+    dist = None
+    if n_ranks > 1:
+        import torch.distributed as dist  # noqa: F811
+        import datetime
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    import torch
+    torch.cuda.set_device(local_rank)
+    flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{local_rank}")
+
+    w, g, grp, queries = make_workload(args.workload)
+    eng = G.Engine(local_rank, max_batch=min(args.batch, 64), profile_kernels=1)
+    dg = eng.graph(g, grp)
+    B = args.batch
+    # each rank takes its own slice of the query stream (replicas, weak scaling)
+    def batch(step):
+        base = ((step * n_ranks + rank) * B) % len(queries)
+        return [queries[(base + i) % len(queries)] for i in range(B)]
+
+    for s in range(args.warmup):
+        dg.solve_batch(batch(s))
+
+    dev_ms, host_ms, lat, stats = [], [], [], []
+    h2d = d2h = launches = 0
+    grow_ms = relax = items = 0.0
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with Clocks(local_rank) as clk:
+        for s in range(args.steps):
+            flush.fill_(s & 0xFF)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ans = dg.solve_batch(batch(args.warmup + s))
+            host_ms.append(1e3 * (time.perf_counter() - t0))
+            st = ans[0].stats
+            dev_ms.append(st["device_ms"])
+            bad = [a for a in ans if a.status not in (G.OK, G.INFEASIBLE)]
+            if bad:
+                raise SystemExit(f"bench: query failed: {G.STATUS[bad[0].status]} {eng.error()}")
+            lat += [a.stats["latency_ms"] for a in ans]
+            h2d += st["h2d_bytes"]
+            d2h += st["d2h_bytes"]
+            launches += st["kernel_launches"]
+            grow_ms += st["grow_ms"]
+            relax += sum(a.stats["edge_relaxations"] for a in ans)
+            items += sum(a.stats["states_expanded"] for a in ans)
+    torch.cuda.synchronize()
+    tot_dev = sum(dev_ms) / 1e3
+    tot_host = sum(host_ms) / 1e3
+    if dist:
+        t = torch.tensor([tot_dev, tot_host], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot_dev, tot_host = float(t[0]), float(t[1])
+    nq_all = args.steps * B * n_ranks
+    value = nq_all / tot_dev
+    e2e = nq_all / tot_host
+
+    # one query at a time, same engine (the reference drivers' mode)
+    per_q = []
+    if rank == 0:
+        for q in queries[: args.single]:
+            a = dg.solve(q)
+            per_q.append(a.stats["device_ms"])
+    peak, peak_kind = peak_hbm()
+    alg_bytes = 24.0 * items + 16.0 * relax
+    grow_launches = max(1, launches // 7)
+    achieved = alg_bytes / (grow_ms / 1e3) / 1e9 if grow_ms > 0 else 0.0
+    line = {
+        "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": n_ranks,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_dev / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic",
+        "config": {"workload": w["name"], "V": g.V, "E_directed": g.E, "global_batch": B * n_ranks,
+                   "k": [q[0] for q in w["queries"]], "parallelism": f"replicas{n_ranks}",
+                   "l2": "flushed between steps (512 MB write)"},
+        "e2e": {"value": e2e, "unit": "queries/s", "h2d_bytes_per_step": h2d // args.steps,
+                "d2h_bytes_per_step": d2h // args.steps},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                       "note": "batched: call start to result ready"},
+        "per_query": {"value": (len(per_q) / (sum(per_q) / 1e3)) if per_q else None,
+                      "unit": "queries/s",
+                      "p50_ms": float(np.percentile(per_q, 50)) if per_q else None,
+                      "p99_ms": float(np.percentile(per_q, 99)) if per_q else None,
+                      "queries": len(per_q)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "kernel": "k_grow",
+                     "peak_kind": peak_kind,
+                     "alg_bytes": alg_bytes, "kernel_ms": grow_ms},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and n_ranks == 1 and not args.no_cpu:
+        res = cpu_reference_sample(w, g, grp, queries[:8], "PrunedDP++", 20.0,
+                                   "; PrunedDP++, 1 thread")
+        if res:
+            qps, loop, done, sample = res
+            line["cpu_baseline"] = {"value": qps, "unit": "queries/s", "cores": 1,
+                                    "kind": "reference", "sample": sample,
+                                    "main_loop_s_per_query": loop}
+    if rank == 0:
+        print(json.dumps(line))
+    dg.close()
+    eng.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--batch", type=int, default=32)
+    ap.add_argument("--single", type=int, default=32, help="queries timed one at a time")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

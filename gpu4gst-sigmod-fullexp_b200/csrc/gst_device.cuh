@@ -443,7 +443,9 @@ __global__ void __launch_bounds__(256) k_rows(Ctx* ctxs, int nctx, DevGraph G, i
         x = __ldcg(row + i);
         buf[i] = x;
       }
-      const uint32_t bal = __ballot_sync(0xffffffffu, i < RW && ((uint32_t)x & PEND));
+      // an unreached cell is all ones, so its pending bit must be ignored
+      const uint32_t bal =
+          __ballot_sync(0xffffffffu, i < RW && x != CELL_INF && ((uint32_t)x & PEND));
       if (lane == 0) pend[i0 >> 5] = bal;
     }
     if (lane == 0) atomicAnd(&c->rowbits[v >> 5], ~(1u << (v & 31)));

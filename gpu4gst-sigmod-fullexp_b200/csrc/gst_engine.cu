@@ -45,11 +45,20 @@ struct Slot {
 
 }  // namespace
 
+// Counters of one gst_solve_batch call.
+struct CallStats {
+  int64_t launches = 0, h2d = 0, d2h = 0;
+  std::vector<std::pair<int, int>> prof;  // (kernel kind, event-pair index)
+  size_t next_ev = 0;
+};
+
 struct gst_engine {
   int device = 0;
   gst_config cfg{};
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<cudaEvent_t> prof_events;  // reused pairs for cfg.profile_kernels
+  CallStats cs;
   int sms = 148;
   int grow_blocks = 0, sssp_blocks = 0;
   std::string err;
@@ -218,22 +227,49 @@ struct LoopShape {
   int rw_max = 1;
 };
 
+enum ProfKind { PROF_GROW = 0, PROF_ROWS = 1, PROF_SSSP = 2 };
+
+// Record the start event of a profiled launch; returns the pair index or -1.
+int prof_begin(gst_engine* eng, int kind) {
+  if (!((eng->cfg.profile_kernels >> kind) & 1)) return -1;
+  const size_t i = eng->cs.next_ev++;
+  while (eng->prof_events.size() < 2 * (i + 1)) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return -1;
+    eng->prof_events.push_back(e);
+  }
+  cudaEventRecord(eng->prof_events[2 * i], eng->stream);
+  eng->cs.prof.push_back({kind, (int)i});
+  return (int)i;
+}
+void prof_end(gst_engine* eng, int i) {
+  if (i >= 0) cudaEventRecord(eng->prof_events[2 * i + 1], eng->stream);
+}
+
 gst_status launch_level(gst_engine* eng, gst_graph* g, int nctx, const LoopShape& sh) {
   cudaStream_t st = eng->stream;
   DevGraph G{g->V, g->E, g->d_beg, g->d_edges};
   const int split = eng->cfg.split_degree;
   const int tpb = eng->cfg.threads_per_block;
   if (sh.sssp) {
+    const int pe = prof_begin(eng, PROF_SSSP);
     k_sssp<<<eng->sssp_blocks, 256, 0, st>>>(g->d_ctx, nctx, G, split);
+    prof_end(eng, pe);
     k_ctrl<<<1, MAXB, 0, st>>>(g->d_ctx, nctx, CTRL_SSSP);
+    eng->cs.launches += 2;
   }
   const size_t per_warp = rows_smem_per_warp(sh.rw_max);
   const int warps = std::max(1, tpb / 32);
+  int pe = prof_begin(eng, PROF_ROWS);
   k_rows<<<eng->grow_blocks, warps * 32, per_warp * warps, st>>>(g->d_ctx, nctx, G, split,
                                                                   sh.rw_max);
+  prof_end(eng, pe);
   k_ctrl<<<1, MAXB, 0, st>>>(g->d_ctx, nctx, CTRL_DP_ROWS);
+  pe = prof_begin(eng, PROF_GROW);
   k_grow<<<eng->grow_blocks, 256, 0, st>>>(g->d_ctx, nctx, G, split);
+  prof_end(eng, pe);
   k_ctrl<<<1, MAXB, 0, st>>>(g->d_ctx, nctx, CTRL_DP_GROW);
+  eng->cs.launches += 4;
   CK(cudaGetLastError());
   return GST_OK;
 }
@@ -352,6 +388,7 @@ gst_status gst_engine_destroy(gst_engine* eng) {
   if (eng->stream) cudaStreamDestroy(eng->stream);
   if (eng->ev0) cudaEventDestroy(eng->ev0);
   if (eng->ev1) cudaEventDestroy(eng->ev1);
+  for (auto e : eng->prof_events) cudaEventDestroy(e);
   delete eng;
   return GST_OK;
 }
@@ -529,6 +566,9 @@ gst_status gst_solve_batch(gst_graph* g, gst_groups* grp, int32_t n, const gst_q
     while (next < n && results[next].status != 0) next++;
     return next < n ? next++ : -1;
   };
+  eng->cs = CallStats();
+  const auto t_call = std::chrono::steady_clock::now();
+  std::vector<double> lat(n > 0 ? n : 1, 0.0);
   CK(cudaEventRecord(eng->ev0, eng->stream));
   int active = 0;
   // fill and run in waves of refills: a finished slot is refilled at the next check
@@ -544,6 +584,8 @@ gst_status gst_solve_batch(gst_graph* g, gst_groups* grp, int32_t n, const gst_q
       gst_status st = reset_slot(eng, g, sl, (size_t)hc.RW, hc.use_lb != 0);
       if (st != GST_OK) return st;
       CK(cudaMemcpyAsync(g->d_ctx + s, &hc, sizeof(Ctx), cudaMemcpyHostToDevice, eng->stream));
+      eng->cs.h2d += sizeof(Ctx);
+      eng->cs.launches += 2;
       // k_init for this slot alone: grid.y selects the context
       DevGraph G{g->V, g->E, g->d_beg, g->d_edges};
       k_init<<<dim3(64, 1), 256, 0, eng->stream>>>(g->d_ctx + s, 1, G, grp->d_ptr, grp->d_mem,
@@ -561,6 +603,7 @@ gst_status gst_solve_batch(gst_graph* g, gst_groups* grp, int32_t n, const gst_q
         idle.phase = PH_DONE;
         idle.best = ~0ull;
         CK(cudaMemcpyAsync(g->d_ctx + s, &idle, sizeof(Ctx), cudaMemcpyHostToDevice, eng->stream));
+        eng->cs.h2d += sizeof(Ctx);
       }
     LoopShape sh;
     sh.sssp = true;
@@ -575,6 +618,7 @@ gst_status gst_solve_batch(gst_graph* g, gst_groups* grp, int32_t n, const gst_q
       }
       CK(cudaMemcpyAsync(g->h_ctx, g->d_ctx, sizeof(Ctx) * nslots, cudaMemcpyDeviceToHost,
                          eng->stream));
+      eng->cs.d2h += (int64_t)sizeof(Ctx) * nslots;
       CK(cudaStreamSynchronize(eng->stream));
       bool any_sssp = false;
       for (int s = 0; s < nslots; s++) {
@@ -587,8 +631,10 @@ gst_status gst_solve_batch(gst_graph* g, gst_groups* grp, int32_t n, const gst_q
     // harvest finished queries
     DevGraph G{g->V, g->E, g->d_beg, g->d_edges};
     k_extract<<<1, MAXB, 0, eng->stream>>>(g->d_ctx, nslots, G);
+    eng->cs.launches += 1;
     CK(cudaMemcpyAsync(g->h_ctx, g->d_ctx, sizeof(Ctx) * nslots, cudaMemcpyDeviceToHost,
                        eng->stream));
+    eng->cs.d2h += (int64_t)sizeof(Ctx) * nslots;
     CK(cudaStreamSynchronize(eng->stream));
     for (int s = 0; s < nslots; s++) {
       if (owner[s] < 0 || g->h_ctx[s].phase < PH_DONE) continue;
@@ -597,6 +643,7 @@ gst_status gst_solve_batch(gst_graph* g, gst_groups* grp, int32_t n, const gst_q
       if (nout) {
         CK(cudaMemcpyAsync(raw.data(), g->slots[s].out, (size_t)nout * 12,
                            cudaMemcpyDeviceToHost, eng->stream));
+        eng->cs.d2h += (int64_t)nout * 12;
         CK(cudaStreamSynchronize(eng->stream));
       }
       fill_result(g, c, &queries[owner[s]], raw, &results[owner[s]]);
@@ -606,7 +653,9 @@ gst_status gst_solve_batch(gst_graph* g, gst_groups* grp, int32_t n, const gst_q
                  owner[s], c.phase, c.error, c.bad_site, c.levels);
         fail(eng, (gst_status)results[owner[s]].status, msg);
       }
-      if (c.error & ERR_EXTRACT) results[owner[s]].status = GST_CAPACITY;
+      if (c.error & ERR_EXTRACT) results[owner[s]].status = GST_DEVICE_ERROR;
+      lat[owner[s]] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() -
+                                                               t_call).count();
       owner[s] = -1;
       active--;
     }
@@ -615,7 +664,24 @@ gst_status gst_solve_batch(gst_graph* g, gst_groups* grp, int32_t n, const gst_q
   CK(cudaEventSynchronize(eng->ev1));
   float ms = 0;
   cudaEventElapsedTime(&ms, eng->ev0, eng->ev1);
-  for (int32_t i = 0; i < n; i++) results[i].stats.device_ms = ms;
+  double kms[3] = {0, 0, 0};
+  for (auto& pr : eng->cs.prof) {
+    float e = 0;
+    if (cudaEventElapsedTime(&e, eng->prof_events[2 * pr.second],
+                             eng->prof_events[2 * pr.second + 1]) == cudaSuccess)
+      kms[pr.first] += e;
+  }
+  for (int32_t i = 0; i < n; i++) {
+    gst_stats& st = results[i].stats;
+    st.device_ms = ms;
+    st.latency_ms = lat[i];
+    st.kernel_launches = eng->cs.launches;
+    st.h2d_bytes = eng->cs.h2d;
+    st.d2h_bytes = eng->cs.d2h;
+    st.grow_ms = kms[PROF_GROW];
+    st.rows_ms = kms[PROF_ROWS];
+    st.sssp_ms = kms[PROF_SSSP];
+  }
   return GST_OK;
 }
 

@@ -270,7 +270,8 @@ class Config(C.Structure):
     _fields_ = [("mem_budget_bytes", C.c_int64), ("split_degree", C.c_int32),
                 ("bucket_delta", C.c_int32), ("max_levels", C.c_int32),
                 ("threads_per_block", C.c_int32), ("blocks_per_sm", C.c_int32),
-                ("max_batch", C.c_int32), ("use_graphs", C.c_int32), ("verbose", C.c_int32)]
+                ("max_batch", C.c_int32), ("use_graphs", C.c_int32),
+                ("profile_kernels", C.c_int32), ("verbose", C.c_int32)]
 
 
 class Query(C.Structure):
@@ -282,7 +283,9 @@ class Stats(C.Structure):
     _fields_ = [("levels", C.c_int64), ("states_expanded", C.c_int64),
                 ("edge_relaxations", C.c_int64), ("merge_pairs", C.c_int64),
                 ("rows_merged", C.c_int64), ("sssp_relaxations", C.c_int64),
-                ("device_ms", C.c_double)]
+                ("kernel_launches", C.c_int64), ("h2d_bytes", C.c_int64),
+                ("d2h_bytes", C.c_int64), ("device_ms", C.c_double), ("latency_ms", C.c_double),
+                ("grow_ms", C.c_double), ("rows_ms", C.c_double), ("sssp_ms", C.c_double)]
 
 
 class Result(C.Structure):

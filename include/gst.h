@@ -63,6 +63,8 @@ typedef struct gst_config {
   int32_t blocks_per_sm;      /* resident CTAs per SM for the level kernels */
   int32_t max_batch;          /* queries resident at once in gst_solve_batch / serving */
   int32_t use_graphs;         /* 1: run the level loop as a CUDA graph with a device-side while node */
+  int32_t profile_kernels;    /* bit0 grow, bit1 rows, bit2 sssp: bracket those launches with
+                                 CUDA events and report their summed device time */
   int32_t verbose;
 } gst_config;
 
@@ -80,7 +82,14 @@ typedef struct gst_stats {
   int64_t merge_pairs;      /* merge pairs evaluated */
   int64_t rows_merged;      /* vertex rows run through the merge closure */
   int64_t sssp_relaxations; /* one-label distance relaxations */
+  int64_t kernel_launches;  /* engine kernels launched (batch: for the whole batch) */
+  int64_t h2d_bytes;        /* host->device bytes moved for the call (batch: whole batch) */
+  int64_t d2h_bytes;        /* device->host bytes moved for the call (batch: whole batch) */
   double device_ms;         /* device time of the query (batch: of the whole batch) */
+  double latency_ms;        /* host time from the call's start to this result being ready */
+  double grow_ms;           /* profiled device time of the grow / rows / sssp launches */
+  double rows_ms;           /*   (batch totals; 0 unless cfg.profile_kernels selects them) */
+  double sssp_ms;
 } gst_stats;
 
 typedef struct gst_result {

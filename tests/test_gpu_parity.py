@@ -1,0 +1,94 @@
+"""Engine parity on the GPU: optimal costs bit-exact against the reference's own
+CPU solvers (golden fixtures) and the oracle, every returned tree verified
+(connected, covers the queried groups, hop-feasible, weight sum == cost)."""
+import numpy as np
+import pytest
+
+import gst_b200 as G
+import oracle as O
+from conftest import golden_inputs, known_answer_graphs, load_golden
+
+pytestmark = pytest.mark.gpu
+REF_INF = 100000
+
+
+def _ref(c):
+    return -1 if c >= REF_INF else c
+
+
+def _check(g, grp, q, hop, a, expect):
+    got = a.cost if a.ok else (-1 if a.status == G.INFEASIBLE else None)
+    assert got == expect, (q, hop, G.STATUS[a.status], a.cost, expect)
+    if a.ok:
+        rc = G.verify_tree(g, grp, q, -1 if hop is None else hop, a.cost, a.edges, a.root)
+        assert rc == 0, (q, hop, G.VERIFY_CODES[rc])
+
+
+@pytest.mark.parametrize("name", ["c1_ba20k_k3", "rmat3k_k4_k5", "rmat20k_k6"])
+def test_engine_matches_reference_golden(engine, name):
+    fx = load_golden(name)
+    g, grp = golden_inputs(fx)
+    dg = engine.graph(g, grp)
+    try:
+        for case in fx["cases"]:
+            hop = case["hop"]
+            costs = next(iter(case["ref"].values()))
+            for q, c in zip(case["queries"], costs):
+                _check(g, grp, q, hop, dg.solve(q, hop), _ref(c))
+    finally:
+        dg.close()
+
+
+def test_engine_known_answers(engine):
+    for g, grp, cases in known_answer_graphs():
+        dg = engine.graph(g, grp)
+        for c in cases:
+            _check(g, grp, c["q"], c["hop"], dg.solve(c["q"], c["hop"]), c["cost"])
+        dg.close()
+
+
+def test_engine_matches_oracle_random(engine):
+    rng = np.random.default_rng(5)
+    for trial in range(4):
+        g = G.synth_rmat(1500 + 500 * trial, 6000 + 3000 * trial, 100 + trial)
+        grp = G.synth_groups_zipf(g.V, 120, 1.5, 2, 60, 200 + trial)
+        dg = engine.graph(g, grp)
+        for k in (1, 2, 3, 5, 6):
+            qs = G.synth_queries(grp.n_groups, 4, k, 300 + trial * 10 + k)
+            for q in qs:
+                hop = None if rng.random() < 0.5 else int(rng.integers(1, 5))
+                o = O.gst_nonhop(g, grp, q) if hop is None else O.gst_hop(g, grp, q, hop)
+                _check(g, grp, q, hop, dg.solve(q, hop), o["cost"])
+        dg.close()
+
+
+def test_batch_equals_single(engine):
+    """Each result is the same alone and in the mix (continuous batching refills
+    slots at level boundaries while other queries are in flight)."""
+    fx = load_golden("rmat3k_k4_k5")
+    g, grp = golden_inputs(fx)
+    dg = engine.graph(g, grp)
+    qs, hops = [], []
+    for case in fx["cases"]:
+        for q in case["queries"][:12]:
+            qs.append(q)
+            hops.append(case["hop"])
+    single = [dg.solve(q, h) for q, h in zip(qs, hops)]
+    mixed = dg.solve_batch(qs, hops)
+    for q, h, a, b in zip(qs, hops, single, mixed):
+        assert a.status == b.status and (not a.ok or a.cost == b.cost), (q, h)
+        if b.ok:
+            assert G.verify_tree(g, grp, q, -1 if h is None else h, b.cost, b.edges, b.root) == 0
+    dg.close()
+
+
+def test_bad_input_is_reported(engine):
+    g = G.synth_ba(200, 2, 1)
+    grp = G.synth_groups_uniform(g.V, 10, 2, 5, 2)
+    dg = engine.graph(g, grp)
+    assert dg.solve([0, 0]).status == G.BAD_INPUT        # duplicate group
+    assert dg.solve([0, 99]).status == G.BAD_INPUT       # unknown group
+    assert dg.solve(list(range(9))).status == G.BAD_INPUT  # k > 8
+    res = dg.solve_batch([[0, 1], [0, 0], [2, 3]])
+    assert res[1].status == G.BAD_INPUT and res[0].ok and res[2].ok
+    dg.close()
