@@ -732,3 +732,282 @@ void gst_result_free(gst_result* r) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// No-allocation solve.
+//
+// Some callers cannot let a library call cudaMalloc: a host application that
+// owns all device memory through its own pool (a database engine's GPU memory
+// manager, a framework's caching allocator, a serving process that carves HBM up
+// front) forbids stray allocations, and cudaMalloc / cudaFree also synchronise
+// the device, stalling the caller's other streams.  gst_solve_noalloc serves
+// them: the caller passes the graph and groups already in device memory and
+// host buffers for the tree; every scratch buffer of the solve (query context,
+// state table, one-label distances, worklists, extraction stack) lives in the
+// file-scope array below, which the CUDA module reserves when it is loaded and
+// keeps until the process exits — on every GPU that loads this library.
+//
+// The array is shared by every call on a device and keeps the previous call's
+// contents; each call clears the parts that must start empty (state table,
+// distances, dirty-row bitmap) before its kernels run.  Two calls whose work
+// overlaps on the same GPU (different streams or host threads) race on the array
+// and corrupt each other: serialise them.  The first call on a device looks up
+// the array's device address (cudaGetSymbolAddress, with that device current)
+// and caches it; make that first call before any stream capture.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kNoallocScratchBytes = (size_t)64 << 20;  // GST_NOALLOC_SCRATCH_BYTES
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kMaxDevices] = {nullptr};
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Device address of the scratch array on `device` (must be current).  Host code
+// cannot use the symbol itself: on the host it names a stand-in object, not
+// device memory.
+gst_status noalloc_scratch(int device, void** out) {
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[device]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) {
+      tl_err = std::string("noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e);
+      return GST_DEVICE_ERROR;
+    }
+    g_noalloc_ptr[device] = p;
+  }
+  *out = g_noalloc_ptr[device];
+  return GST_OK;
+}
+
+gst_status noalloc_fail(gst_status s, const char* msg) {
+  tl_err = msg;
+  return s;
+}
+
+gst_status noalloc_solve(int device, cudaStream_t st, int64_t V, int64_t E, const int64_t* d_beg,
+                         const int32_t* d_edges, int32_t n_groups, const int64_t* d_grp_ptr,
+                         const int32_t* d_members, const gst_query* q, int64_t edge_cap,
+                         gst_result* res) {
+  gst_engine* eng = nullptr;  // for CK()
+  if (!res) return noalloc_fail(GST_BAD_INPUT, "noalloc: null result");
+  int32_t* eu = res->edge_u;
+  int32_t* ev = res->edge_v;
+  int32_t* ew = res->edge_w;
+  memset(res, 0, sizeof(*res));
+  res->edge_u = eu;
+  res->edge_v = ev;
+  res->edge_w = ew;
+  if (!q || !d_beg || !d_grp_ptr || !d_members || (E > 0 && !d_edges) || V < 1 ||
+      V >= ((int64_t)1 << 27) || E < 0 || n_groups < 1 || edge_cap < 0 ||
+      (edge_cap > 0 && (!eu || !ev || !ew)))
+    return noalloc_fail(GST_BAD_INPUT, "noalloc: bad arguments");
+  res->user_tag = q->user_tag;
+  if (q->k < 1 || q->k > KMAX || !q->group_ids || q->hop_bound > 30)
+    return res->status = GST_BAD_INPUT,
+           noalloc_fail(GST_BAD_INPUT, "noalloc: k must be in [1,8], hop bound <= 30");
+  for (int i = 0; i < q->k; i++) {
+    const int32_t a = q->group_ids[i];
+    if (a < 0 || a >= n_groups)
+      return res->status = GST_BAD_INPUT, noalloc_fail(GST_BAD_INPUT, "noalloc: group id out of range");
+    for (int j = 0; j < i; j++)
+      if (q->group_ids[j] == a)
+        return res->status = GST_BAD_INPUT, noalloc_fail(GST_BAD_INPUT, "noalloc: duplicate group id");
+  }
+  // scratch layout; reject what does not fit
+  const int hop = q->hop_bound >= 0;
+  const size_t RW = row_width(q->k, q->hop_bound);
+  const uint32_t outcap = 1u << 14, stackcap = 1u << 16;
+  size_t off = align256(sizeof(Ctx));
+  const size_t o_table = off;
+  off = align256(off + (size_t)V * RW * 8);
+  const size_t o_dist = off;
+  off = align256(off + (size_t)V * DIST_STRIDE * 4);
+  const size_t o_bits = off;
+  off = align256(off + ((size_t)V + 31) / 32 * 4);
+  const size_t o_rows = off;
+  off = align256(off + (size_t)V * 4);
+  const size_t o_out = off;
+  off = align256(off + (size_t)outcap * 12);
+  const size_t o_stack = off;
+  off = align256(off + (size_t)stackcap * 8);
+  const size_t min_lists = 4 * (size_t)(4 * V + 4096) * 16;
+  if (off + min_lists > kNoallocScratchBytes) {
+    char msg[200];
+    snprintf(msg, sizeof msg,
+             "noalloc: this query needs more than the %zu-byte static scratch "
+             "(V=%lld, row width %zu); use gst_solve",
+             kNoallocScratchBytes, (long long)V, RW);
+    res->status = GST_OOM_ADMISSION;
+    return noalloc_fail(GST_OOM_ADMISSION, msg);
+  }
+  const uint64_t want = (uint64_t)V * RW + 4ull * (uint64_t)V + 4096;
+  const uint64_t fit = (kNoallocScratchBytes - off) / (4 * 16);
+  const uint32_t cap = (uint32_t)std::min<uint64_t>(std::min<uint64_t>(want, fit), 1ull << 26);
+
+  int prev_dev = 0;
+  CK(cudaGetDevice(&prev_dev));
+  CK(cudaSetDevice(device));
+  void* scratch = nullptr;
+  gst_status s = noalloc_scratch(device, &scratch);
+  if (s != GST_OK) {
+    cudaSetDevice(prev_dev);
+    res->status = s;
+    return s;
+  }
+  unsigned char* base = (unsigned char*)scratch;
+  // empty-group check: members of each queried group
+  for (int i = 0; i < q->k; i++) {
+    int64_t be[2];
+    CK(cudaMemcpyAsync(be, d_grp_ptr + q->group_ids[i], sizeof(be), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (be[1] <= be[0]) {
+      cudaSetDevice(prev_dev);
+      res->status = GST_BAD_INPUT;
+      return noalloc_fail(GST_BAD_INPUT, "noalloc: group has no members");
+    }
+  }
+  int sms = 148;
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  gst_config cfg;
+  gst_config_default(&cfg);
+  const int split = cfg.split_degree;
+  Ctx c;
+  memset(&c, 0, sizeof(c));
+  c.table = (uint64_t*)(base + o_table);
+  c.dist = (uint32_t*)(base + o_dist);
+  c.rowbits = (uint32_t*)(base + o_bits);
+  c.q[0] = (uint4*)(base + off);
+  c.q[1] = (uint4*)(base + off + (size_t)cap * 16);
+  c.far[0] = (uint4*)(base + off + 2 * (size_t)cap * 16);
+  c.far[1] = (uint4*)(base + off + 3 * (size_t)cap * 16);
+  c.rows = (uint32_t*)(base + o_rows);
+  c.out = (int32_t*)(base + o_out);
+  c.stack = (uint64_t*)(base + o_stack);
+  c.qcap = c.farcap = cap;
+  c.rowcap = (uint32_t)V;
+  c.outcap = outcap;
+  c.stackcap = stackcap;
+  c.k = q->k;
+  c.W = 1 << q->k;
+  c.full = c.W - 1;
+  c.D = hop ? q->hop_bound : 0;
+  c.DD = hop ? q->hop_bound + 1 : 1;
+  c.RW = c.W * c.DD;
+  c.hop = hop;
+  c.use_lb = hop ? 0 : 1;
+  for (int i = 0; i < q->k; i++) c.gid[i] = q->group_ids[i];
+  c.delta = 0;
+  c.max_levels = (uint32_t)cfg.max_levels;
+  c.in_idx = 1;
+  c.far_min = 0xFFFFFFFFu;
+  c.bucket_end = 0xFFFFFFFFu;
+  c.ub = 0xFFFFFFFFu;
+  c.ub_cell = 0xFFFFFFFFu;
+  c.best = ~0ull;
+  c.phase = c.use_lb ? PH_SSSP : PH_DP;
+  Ctx* d_ctx = (Ctx*)base;
+  // clear what must start empty, then upload the context
+  CK(cudaMemsetAsync(c.table, 0xFF, (size_t)V * RW * 8, st));
+  CK(cudaMemsetAsync(c.dist, 0xFF, (size_t)V * DIST_STRIDE * 4, st));
+  CK(cudaMemsetAsync(c.rowbits, 0, ((size_t)V + 31) / 32 * 4, st));
+  CK(cudaMemcpyAsync(d_ctx, &c, sizeof(Ctx), cudaMemcpyHostToDevice, st));
+  DevGraph G{V, E, d_beg, (const int2*)d_edges};
+  k_init<<<dim3(64, 1), 256, 0, st>>>(d_ctx, 1, G, d_grp_ptr, d_members, split);
+  k_ctrl<<<1, 32, 0, st>>>(d_ctx, 1, CTRL_SSSP);
+  const int blocks = sms * cfg.blocks_per_sm;
+  const size_t per_warp = rows_smem_per_warp((int)RW);
+  const int warps = cfg.threads_per_block / 32;
+  cudaFuncSetAttribute(k_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  int64_t launches = 2;
+  Ctx h;
+  const auto t0 = std::chrono::steady_clock::now();
+  for (;;) {
+    for (int i = 0; i < 6; i++) {
+      k_sssp<<<blocks, 256, 0, st>>>(d_ctx, 1, G, split);
+      k_ctrl<<<1, 32, 0, st>>>(d_ctx, 1, CTRL_SSSP);
+      k_rows<<<blocks, warps * 32, per_warp * warps, st>>>(d_ctx, 1, G, split, (int)RW);
+      k_ctrl<<<1, 32, 0, st>>>(d_ctx, 1, CTRL_DP_ROWS);
+      k_grow<<<blocks, 256, 0, st>>>(d_ctx, 1, G, split);
+      k_ctrl<<<1, 32, 0, st>>>(d_ctx, 1, CTRL_DP_GROW);
+      launches += 6;
+    }
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(&h, d_ctx, sizeof(Ctx), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (h.phase >= PH_DONE) break;
+  }
+  k_extract<<<1, 32, 0, st>>>(d_ctx, 1, G);
+  launches++;
+  CK(cudaMemcpyAsync(&h, d_ctx, sizeof(Ctx), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  res->status = status_of(h);
+  if (h.error & ERR_EXTRACT) res->status = GST_DEVICE_ERROR;
+  res->stats.levels = h.levels;
+  res->stats.states_expanded = (int64_t)h.st_items;
+  res->stats.edge_relaxations = (int64_t)h.st_relax;
+  res->stats.merge_pairs = (int64_t)h.st_merge;
+  res->stats.rows_merged = (int64_t)h.st_rows;
+  res->stats.sssp_relaxations = (int64_t)h.st_sssp;
+  res->stats.kernel_launches = launches;
+  res->stats.latency_ms =
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  res->stats.device_ms = res->stats.latency_ms;
+  if (res->status == GST_OK) {
+    res->cost = (int32_t)(h.best >> 32);
+    res->root = (int32_t)(h.best & 0x7FFFFFFull);
+    res->root_hop = (int32_t)((h.best >> 27) & 31u);
+    const int64_t nraw = std::min<int64_t>(h.n_out, outcap);
+    if (nraw > edge_cap) {
+      res->status = GST_CAPACITY;
+    } else if (nraw > 0) {
+      // scatter the interleaved (u, v, w) triples into the caller's three arrays
+      CK(cudaMemcpy2DAsync(eu, 4, c.out + 0, 12, 4, (size_t)nraw, cudaMemcpyDeviceToHost, st));
+      CK(cudaMemcpy2DAsync(ev, 4, c.out + 1, 12, 4, (size_t)nraw, cudaMemcpyDeviceToHost, st));
+      CK(cudaMemcpy2DAsync(ew, 4, c.out + 2, 12, 4, (size_t)nraw, cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      // in place: orient u < v, drop repeated edges, sort by (u, v)
+      int64_t m = 0;
+      for (int64_t i = 0; i < nraw; i++) {
+        int32_t a = eu[i], b = ev[i];
+        if (a > b) std::swap(a, b);
+        bool dup = false;
+        for (int64_t j = 0; j < m && !dup; j++) dup = eu[j] == a && ev[j] == b;
+        if (dup) continue;
+        const int32_t w = ew[i];
+        int64_t p = m++;
+        while (p > 0 && (eu[p - 1] > a || (eu[p - 1] == a && ev[p - 1] > b))) {
+          eu[p] = eu[p - 1];
+          ev[p] = ev[p - 1];
+          ew[p] = ew[p - 1];
+          p--;
+        }
+        eu[p] = a;
+        ev[p] = b;
+        ew[p] = w;
+      }
+      res->n_edges = m;
+    }
+  }
+  cudaSetDevice(prev_dev);
+  return res->status == GST_OK ? GST_OK : (gst_status)res->status;
+}
+
+}  // namespace
+
+extern "C" gst_status gst_solve_noalloc(int32_t device, void* stream, int64_t V, int64_t E,
+                                        const int64_t* d_beg_pos, const int32_t* d_edges,
+                                        int32_t n_groups, const int64_t* d_grp_ptr,
+                                        const int32_t* d_members, const gst_query* q,
+                                        int64_t edge_cap, gst_result* res) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev ||
+      device >= kMaxDevices)
+    return noalloc_fail(GST_BAD_INPUT, "noalloc: bad device");
+  return noalloc_solve(device, (cudaStream_t)stream, V, E, d_beg_pos, d_edges, n_groups,
+                       d_grp_ptr, d_members, q, edge_cap, res);
+}

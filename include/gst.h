@@ -143,6 +143,27 @@ void gst_result_free(gst_result* res);
 gst_status gst_debug_slot_state(gst_graph* g, int32_t slot, uint64_t* cells, int64_t n_cells,
                                 uint64_t* best_out);
 
+/* No-allocation solve (no counterpart in the reference; added for callers that
+ * may not allocate device memory).  Some hosts own all device memory through their
+ * own pool and forbid a library from calling cudaMalloc/cudaFree, which would also
+ * synchronise the device.  This entry point runs one query like gst_solve but
+ * allocates nothing: the graph (d_beg_pos[V+1]; d_edges[2E] = neighbour, weight
+ * interleaved, sorted by neighbour per vertex, weights >= 1) and the groups
+ * (d_grp_ptr[n_groups+1], d_members) are the caller's, already in device memory;
+ * the tree is written into the caller's host arrays res->edge_u/edge_v/edge_w of
+ * edge_cap entries each (do not call gst_result_free on this result).  All scratch
+ * lives in a static device array of GST_NOALLOC_SCRATCH_BYTES that the library
+ * holds on every GPU that loads it until the process exits; a query whose state
+ * table and worklists do not fit is rejected with GST_OOM_ADMISSION.  The first
+ * call on a device looks the array's address up (issue it before any stream
+ * capture).  Calls share the array: calls that overlap on one GPU race, so
+ * serialise them.  `stream` is a cudaStream_t (NULL = legacy default stream). */
+#define GST_NOALLOC_SCRATCH_BYTES (64ll << 20)
+gst_status gst_solve_noalloc(int32_t device, void* stream, int64_t V, int64_t E,
+                             const int64_t* d_beg_pos, const int32_t* d_edges, int32_t n_groups,
+                             const int64_t* d_grp_ptr, const int32_t* d_members,
+                             const gst_query* q, int64_t edge_cap, gst_result* res);
+
 #ifdef __cplusplus
 }
 #endif
