@@ -55,7 +55,7 @@ def build(force: bool = False, verbose_ptxas: bool = False, checked: bool = Fals
         o = os.path.join(BUILD, src + ".o")
         if force or _stale(o, [s] + hdrs):
             cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
-                   "-I", INC, "-I", CSRC, "-c", s, "-o", o]
+                   "-Xcompiler", "-fopenmp", "-I", INC, "-I", CSRC, "-c", s, "-o", o]
             if verbose_ptxas:
                 cmd.insert(1, "-Xptxas=-v")
             _run(cmd)
@@ -84,7 +84,8 @@ def _build_checked(force: bool) -> str:
     for src in CU_SOURCES:
         o = os.path.join(BUILD, src + ".checked.o")
         _run([NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-DGST_CHECKED", "-Xcompiler",
-              "-fPIC", "-I", INC, "-I", CSRC, "-c", os.path.join(CSRC, src), "-o", o])
+              "-fPIC", "-Xcompiler", "-fopenmp", "-I", INC, "-I", CSRC, "-c",
+              os.path.join(CSRC, src), "-o", o])
         objs.append(o)
     build(force)
     objs += [os.path.join(BUILD, s + ".o") for s in CPP_SOURCES]

@@ -50,17 +50,35 @@ constexpr int MAXB = 64;          // queries per batched launch
 constexpr int KMAX = 8;           // groups per query
 constexpr int DIST_STRIDE = 8;    // int32 one-label distances per vertex row
 
-enum Phase : uint32_t { PH_SSSP = 0, PH_DP = 1, PH_DONE = 2, PH_ERROR = 3 };
+// PH_PREP: distances final; the star bound, group distances and tour table are
+// being built (one k_sssp pass over the distance rows, then the control block).
+enum Phase : uint32_t { PH_SSSP = 0, PH_PREP = 1, PH_DP = 2, PH_DONE = 3, PH_ERROR = 4 };
 enum ErrBits : uint32_t { ERR_QCAP = 1, ERR_FARCAP = 2, ERR_ROWCAP = 4, ERR_TIMEOUT = 8,
                           ERR_EXTRACT = 16, ERR_BOUNDS = 32 };
 enum CtrlMode : int { CTRL_SSSP = 0, CTRL_DP_ROWS = 1, CTRL_DP_GROW = 2 };
 
+constexpr int WIDX = 8;            // light-edge index: counts of edges with w <= 2^j, j < 8
+constexpr int TOUR_STRIDE = KMAX * KMAX;
+
 struct DevGraph {
   int64_t V;
   int64_t E;
-  const int64_t* beg;  // V+1
-  const int2* edges;   // E x {neighbour, weight}, sorted by neighbour per vertex
+  const int64_t* beg;     // V+1
+  const int2* edges;      // E x {neighbour, weight}, sorted by neighbour per vertex
+  const int2* wedges;     // the same edges sorted by (weight, neighbour) per vertex
+  const uint32_t* widx;   // V x WIDX: edges of v with weight <= 2^j (NULL: no index,
+                          // wedges then need not be weight-sorted)
 };
+
+// Number of leading entries of v's weight-sorted edge list that can hold an edge
+// of weight <= lim (an over-count by at most the edges in (lim, 2^j]).
+__device__ __forceinline__ int64_t light_count(const DevGraph& G, uint32_t v, int64_t deg,
+                                               uint32_t lim) {
+  if (lim == 0u) return 0;
+  if (!G.widx || lim > (1u << (WIDX - 1))) return deg;
+  const int j = 32 - __clz(lim - 1u);  // smallest j with 2^j >= lim
+  return (int64_t)__ldg(&G.widx[(uint64_t)v * WIDX + j]);
+}
 
 // Per-query context.  Fields above `in_ptr` are written by the host before the
 // query starts; the rest are updated by the control kernel between launches and
@@ -69,6 +87,7 @@ struct Ctx {
   uint64_t* table;
   uint32_t* dist;
   uint32_t* rowbits;
+  uint32_t* tour;      // 2^k x TOUR_STRIDE path table, then 2^k x KMAX row minima
   uint4* q[2];
   uint4* far[2];
   uint32_t* rows;
@@ -76,7 +95,9 @@ struct Ctx {
   uint64_t* stack;     // extraction stack
   uint32_t qcap, farcap, rowcap, outcap, stackcap;
   int32_t k, W, full, D, DD, RW, hop, use_lb;
+  int32_t use_tour;     // tour lower bound (needs use_lb)
   int32_t gid[KMAX];
+  uint32_t vv[KMAX * KMAX];  // group-to-group distances (min over members of i of d_j)
   uint32_t delta;       // bucket width (0 = one bucket)
   uint32_t max_levels;
   // control state
@@ -166,10 +187,11 @@ __device__ __forceinline__ void push_far(Ctx* c, const uint4& e) {
   else atomicOr(&c->error, (uint32_t)ERR_FARCAP);
   atomicMin(&c->far_min, e.z);
 }
-// Emit the work items of state (v, pd) with cost `cost`: one per `split` edges.
+// Emit the work items of state (v, pd) with cost `cost`: one per `split` edges of
+// the first `cnt` entries of v's edge list.
 __device__ __forceinline__ void push_state(Ctx* c, uint32_t v, uint32_t pd, uint32_t cost,
-                                           int64_t deg, int split, uint32_t bucket_end) {
-  const uint32_t nch = (uint32_t)((deg + split - 1) / split);
+                                           int64_t cnt, int split, uint32_t bucket_end) {
+  const uint32_t nch = (uint32_t)((cnt + split - 1) / split);
   const bool near = cost < bucket_end;
   for (uint32_t ch = 0; ch < nch; ch++) {
     const uint4 e = make_uint4(v, pd, cost, ch);
@@ -177,6 +199,17 @@ __device__ __forceinline__ void push_state(Ctx* c, uint32_t v, uint32_t pd, uint
     else push_far(c, e);
   }
 }
+// Largest edge weight a grow step from a state of cost `cost` can still use: a
+// target must stay <= ub (unbounded) or < ub_cell (hop-bounded).
+__device__ __forceinline__ uint32_t grow_limit(const Ctx* c, uint32_t cost) {
+  if (c->hop) {
+    const uint32_t b = c->ub_cell;
+    return b > cost ? b - cost - 1u : 0u;
+  }
+  const uint32_t b = c->ub;
+  return b >= cost ? b - cost : 0u;
+}
+
 __device__ __forceinline__ void mark_row(Ctx* c, uint32_t u) {
   const uint32_t bit = 1u << (u & 31);
   const uint32_t old = atomicOr(&c->rowbits[u >> 5], bit);
@@ -307,7 +340,7 @@ __global__ void __launch_bounds__(256) k_sssp(Ctx* ctxs, int nctx, DevGraph G, i
         const uint32_t off = j - (o_scan - o_n);
         Ctx* c = ctxs + o_qi;
         if (!in_bounds(c, o_eb + off < G.E, 3)) continue;
-        const int2 ed = G.edges[o_eb + off];
+        const int2 ed = G.wedges[o_eb + off];
         const uint32_t u = (uint32_t)ed.x;
         const uint32_t nd = o_cost + (uint32_t)ed.y;
         if (!in_bounds(c, u < G.V, 4)) continue;
@@ -321,6 +354,38 @@ __global__ void __launch_bounds__(256) k_sssp(Ctx* ctxs, int nctx, DevGraph G, i
         }
       }
     }
+  }
+  // Queries whose distances are final (PH_PREP): one pass over the distance rows
+  // gives the star bound min_v sum_i d_i(v) (the cost of the k shortest paths from
+  // the best centre v, a feasible tree, so a valid ub) and the group distances
+  // vv[i][j] = min over members m of group i of d_j(m) (the host loop of
+  // code/TrimCDP-WB/src/GSTnonHop.cu:341-353, done on the device).
+  for (int qi = 0; qi < nctx; qi++) {
+    Ctx* c = ctxs + qi;
+    if (c->phase != PH_PREP) continue;
+    const int k = c->k;
+    uint32_t best = COST_INF;
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < G.V;
+         v += (int64_t)gridDim.x * blockDim.x) {
+      const uint4* row = (const uint4*)&c->dist[(uint64_t)v * DIST_STRIDE];
+      const uint4 a = __ldcg(row), b = __ldcg(row + 1);
+      const uint32_t d[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+      uint64_t sum = 0;
+#pragma unroll
+      for (int i = 0; i < KMAX; i++)
+        if (i < k) sum += d[i];
+      if (sum < best) best = (uint32_t)sum;
+#pragma unroll
+      for (int i = 0; i < KMAX; i++)
+        if (i < k && d[i] == 0u) {
+#pragma unroll
+          for (int j = 0; j < KMAX; j++)
+            if (j < k && d[j] < __ldcg(&c->vv[i * KMAX + j])) atomicMin(&c->vv[i * KMAX + j], d[j]);
+        }
+    }
+    best = __reduce_min_sync(0xffffffffu, best);
+    if ((threadIdx.x & 31) == 0 && best < COST_INF && !c->hop && best < __ldcg(&c->ub))
+      atomicMin(&c->ub, best);
   }
 }
 
@@ -357,8 +422,9 @@ __global__ void __launch_bounds__(256) k_grow(Ctx* ctxs, int nctx, DevGraph G, i
           push_far(c, e);
         } else {
           const int64_t b0 = G.beg[v], b1 = G.beg[v + 1];
+          const int64_t lc = light_count(G, v, b1 - b0, grow_limit(c, cost));
           eb = b0 + (int64_t)e.w * split;
-          const int64_t ee = min(b1, eb + (int64_t)split);
+          const int64_t ee = min(b0 + lc, eb + (int64_t)split);
           n = ee > eb ? (uint32_t)(ee - eb) : 0u;
         }
       }
@@ -381,7 +447,7 @@ __global__ void __launch_bounds__(256) k_grow(Ctx* ctxs, int nctx, DevGraph G, i
         Ctx* c = ctxs + o_qi;
         const uint32_t off = j - (o_scan - o_n);
         if (!in_bounds(c, o_eb + off < G.E, 6)) continue;
-        const int2 ed = G.edges[o_eb + off];
+        const int2 ed = G.wedges[o_eb + off];
         const uint32_t u = (uint32_t)ed.x;
         const uint32_t nc = o_cost + (uint32_t)ed.y;
         if (!in_bounds(c, u < G.V, 7)) continue;
@@ -527,7 +593,39 @@ __global__ void __launch_bounds__(256) k_rows(Ctx* ctxs, int nctx, DevGraph G, i
           const uint32_t bound = hop ? c->ub_cell : c->ub;
           bool grow = 2ull * cst <= (uint64_t)bound && (uint64_t)cst + lb <= (uint64_t)bound;
           if (hop) grow = grow && (int)d < D && cst < bound;
-          if (grow && deg > 0) push_state(c, v, p | (d << 16), cst, deg, split, c->bucket_end);
+          if (grow && c->use_tour) {
+            // tour bound of PrunedDP++ (code/PrunedDP++/include/CPUNONHOP.h:433-493):
+            // the rest of the tree, doubled, is a closed walk from v through every
+            // group of Xb = full \ p, so twice its cost is at least
+            //   min_{i,j} d_i(v) + P(i,j,Xb) + d_j(v)            and, for every i,
+            //   d_i(v) + min_j P(i,j,Xb) + min_j d_j(v),
+            // P = cheapest group sequence from i to j visiting each group of Xb once.
+            const uint32_t Xb = full ^ p;
+            const uint32_t* Wt = c->tour + (size_t)Xb * TOUR_STRIDE;
+            const uint32_t* W2 = c->tour + (size_t)c->W * TOUR_STRIDE + (size_t)Xb * KMAX;
+            uint64_t mind = COST_INF;
+#pragma unroll
+            for (int b = 0; b < KMAX; b++)
+              if (b < k && ((Xb >> b) & 1u) && dv[b] < mind) mind = dv[b];
+            uint64_t lb1 = ~0ull, lb2 = 0;
+#pragma unroll
+            for (int a = 0; a < KMAX; a++) {
+              if (a >= k || !((Xb >> a) & 1u)) continue;
+              const uint64_t t2 = (uint64_t)dv[a] + __ldg(&W2[a]) + mind;
+              if (t2 > lb2) lb2 = t2;
+#pragma unroll
+              for (int b = 0; b < KMAX; b++) {
+                if (b >= k || !((Xb >> b) & 1u)) continue;
+                const uint64_t t1 = (uint64_t)dv[a] + __ldg(&Wt[a * KMAX + b]) + dv[b];
+                if (t1 < lb1) lb1 = t1;
+              }
+            }
+            const uint64_t t = lb1 > lb2 ? lb1 : lb2;
+            grow = (uint64_t)cst + (t + 1) / 2 <= (uint64_t)bound;
+          }
+          if (grow && deg > 0)
+            push_state(c, v, p | (d << 16), cst, light_count(G, v, deg, grow_limit(c, cst)), split,
+                       c->bucket_end);
         }
       }
     }
@@ -554,10 +652,74 @@ __device__ __forceinline__ void ctrl_take_far(Ctx* c) {
   c->far_min = 0xFFFFFFFFu;
 }
 
+// Tour table of one query (all threads of the block): P[X][i][j] = cheapest
+// sequence of group-to-group hops that starts in group i, ends in group j and
+// visits every group of X exactly once (Held-Karp over the vv distances), then the
+// row minima P2[X][i] = min_j P[X][i][j].  The reference builds a closure of the
+// same table on the host (code/TrimCDP-WB/src/GSTnonHop.cu:355-404,
+// code/PrunedDP++/include/CPUNONHOP.h:266-383 and :564-586).
+__device__ void build_tour(Ctx* c) {
+  const int k = c->k, W = c->W;
+  uint32_t* P = c->tour;
+  for (int L = 1; L <= k; L++) {
+    for (int idx = threadIdx.x; idx < W * k; idx += blockDim.x) {
+      const uint32_t X = (uint32_t)(idx / k);
+      const int i = idx - (int)X * k;
+      if (__popc(X) != L || !((X >> i) & 1u)) continue;
+      for (int p = 0; p < k; p++) {
+        if (!((X >> p) & 1u)) continue;
+        uint32_t val = COST_INF;
+        if (L == 1) {
+          val = 0u;  // X == {i}, p == i
+        } else if (p != i) {
+          const uint32_t prev = X ^ (1u << p);
+          for (int j = 0; j < k; j++) {
+            if (!((prev >> j) & 1u)) continue;
+            const uint64_t x = (uint64_t)P[(size_t)prev * TOUR_STRIDE + i * KMAX + j] +
+                               c->vv[j * KMAX + p];
+            if (x < val) val = (uint32_t)x;
+          }
+        }
+        P[(size_t)X * TOUR_STRIDE + i * KMAX + p] = val;
+      }
+    }
+    __syncthreads();
+  }
+  uint32_t* P2 = P + (size_t)W * TOUR_STRIDE;
+  for (int idx = threadIdx.x; idx < W * k; idx += blockDim.x) {
+    const uint32_t X = (uint32_t)(idx / k);
+    const int i = idx - (int)X * k;
+    uint32_t m = COST_INF;
+    if ((X >> i) & 1u)
+      for (int p = 0; p < k; p++)
+        if ((X >> p) & 1u) m = min(m, P[(size_t)X * TOUR_STRIDE + i * KMAX + p]);
+    P2[(size_t)X * KMAX + i] = m;
+  }
+}
+
+// DP start: the first step of the DP is the rows kernel over the seeded rows.
+__device__ __forceinline__ void ctrl_start_dp(Ctx* c) {
+  c->phase = PH_DP;
+  c->in_n = 0;
+  c->no = 0;
+  c->n_q[0] = c->n_q[1] = 0;
+  c->n_far[0] = c->n_far[1] = 0;
+  c->far_min = 0xFFFFFFFFu;
+  c->bucket_end = c->delta ? c->delta : 0xFFFFFFFFu;
+}
+
+// One block per query context; thread 0 runs the control logic, the whole block
+// builds the tour table when a query leaves its distance phase.
 __global__ void k_ctrl(Ctx* ctxs, int nctx, int mode) {
-  const int qi = blockIdx.x * blockDim.x + threadIdx.x;
+  const int qi = blockIdx.x;
   if (qi >= nctx) return;
   Ctx* c = ctxs + qi;
+  if (mode == CTRL_SSSP && c->phase == PH_PREP && !c->error) {
+    if (c->use_tour) build_tour(c);  // block-uniform branch
+    if (threadIdx.x == 0) ctrl_start_dp(c);
+    return;
+  }
+  if (threadIdx.x != 0) return;
   if (c->phase >= PH_DONE) return;
   if (c->error) {
     c->phase = PH_ERROR;
@@ -586,14 +748,10 @@ __global__ void k_ctrl(Ctx* ctxs, int nctx, int mode) {
       ctrl_take_far(c);
       c->no = s;
     } else {
-      // distances final: start the DP (its first step is the rows kernel)
-      c->phase = PH_DP;
+      // distances final: the next k_sssp launch builds the bounds (PH_PREP), the
+      // control step after it the tour table, then the DP starts
+      c->phase = PH_PREP;
       c->in_n = 0;
-      c->no = 0;
-      c->n_q[0] = c->n_q[1] = 0;
-      c->n_far[0] = c->n_far[1] = 0;
-      c->far_min = 0xFFFFFFFFu;
-      c->bucket_end = c->delta ? c->delta : 0xFFFFFFFFu;
     }
   } else if (mode == CTRL_DP_ROWS) {
     if (c->phase != PH_DP) return;

@@ -34,6 +34,7 @@ struct Slot {
   uint64_t* table = nullptr;
   uint32_t* dist = nullptr;
   uint32_t* rowbits = nullptr;
+  uint32_t* tour = nullptr;
   uint4* q[2] = {nullptr, nullptr};
   uint4* far[2] = {nullptr, nullptr};
   uint32_t* rows = nullptr;
@@ -69,7 +70,9 @@ struct gst_graph {
   gst_engine* eng = nullptr;
   int64_t V = 0, E = 0;
   int64_t* d_beg = nullptr;
-  int2* d_edges = nullptr;
+  int2* d_edges = nullptr;   // per vertex sorted by neighbour (tree extraction)
+  int2* d_wedges = nullptr;  // per vertex sorted by (weight, neighbour) (grow, SSSP)
+  uint32_t* d_widx = nullptr;
   std::vector<int64_t> h_beg;
   std::vector<Slot> slots;
   Ctx* d_ctx = nullptr;       // MAXB contexts
@@ -104,6 +107,7 @@ void free_slot(Slot& s) {
   cudaFree(s.table);
   cudaFree(s.dist);
   cudaFree(s.rowbits);
+  cudaFree(s.tour);
   cudaFree(s.q[0]);
   cudaFree(s.q[1]);
   cudaFree(s.far[0]);
@@ -120,9 +124,12 @@ uint32_t list_cap(int64_t V, size_t rw) {
   return (uint32_t)std::min<uint64_t>(want, 1ull << 26);
 }
 
+constexpr size_t kTourWords = ((size_t)1 << KMAX) * (TOUR_STRIDE + KMAX);
+
 size_t slot_bytes(int64_t V, size_t rw) {
   const uint64_t cap = list_cap(V, rw);
   return (size_t)V * rw * 8 + (size_t)V * DIST_STRIDE * 4 + ((size_t)V + 31) / 32 * 4 +
+         kTourWords * 4 +
          4 * (size_t)cap * 16 + (size_t)V * 4 + (size_t)(1 << 16) * 12 + (size_t)(1 << 18) * 8;
 }
 
@@ -141,6 +148,7 @@ gst_status ensure_slot(gst_engine* eng, gst_graph* g, size_t idx, size_t rw) {
   CK(cudaMalloc(&s.table, (size_t)V * rw * 8));
   CK(cudaMalloc(&s.dist, (size_t)V * DIST_STRIDE * 4));
   CK(cudaMalloc(&s.rowbits, ((size_t)V + 31) / 32 * 4));
+  CK(cudaMalloc(&s.tour, kTourWords * 4));
   for (int i = 0; i < 2; i++) {
     CK(cudaMalloc(&s.q[i], (size_t)s.qcap * 16));
     CK(cudaMalloc(&s.far[i], (size_t)s.farcap * 16));
@@ -177,6 +185,7 @@ void prep_ctx(gst_engine* eng, gst_graph* g, Slot& s, const gst_query* q, Ctx& c
   c.table = s.table;
   c.dist = s.dist;
   c.rowbits = s.rowbits;
+  c.tour = s.tour;
   c.q[0] = s.q[0];
   c.q[1] = s.q[1];
   c.far[0] = s.far[0];
@@ -197,7 +206,9 @@ void prep_ctx(gst_engine* eng, gst_graph* g, Slot& s, const gst_query* q, Ctx& c
   c.RW = c.W * c.DD;
   c.hop = hop;
   c.use_lb = hop ? 0 : 1;
+  c.use_tour = c.use_lb;
   for (int i = 0; i < q->k; i++) c.gid[i] = q->group_ids[i];
+  memset(c.vv, 0xFF, sizeof(c.vv));
   c.delta = (uint32_t)std::max(0, eng->cfg.bucket_delta);
   c.max_levels = (uint32_t)eng->cfg.max_levels;
   c.in_ptr = nullptr;
@@ -246,16 +257,20 @@ void prof_end(gst_engine* eng, int i) {
   if (i >= 0) cudaEventRecord(eng->prof_events[2 * i + 1], eng->stream);
 }
 
+DevGraph dev_graph(const gst_graph* g) {
+  return DevGraph{g->V, g->E, g->d_beg, g->d_edges, g->d_wedges, g->d_widx};
+}
+
 gst_status launch_level(gst_engine* eng, gst_graph* g, int nctx, const LoopShape& sh) {
   cudaStream_t st = eng->stream;
-  DevGraph G{g->V, g->E, g->d_beg, g->d_edges};
+  const DevGraph G = dev_graph(g);
   const int split = eng->cfg.split_degree;
   const int tpb = eng->cfg.threads_per_block;
   if (sh.sssp) {
     const int pe = prof_begin(eng, PROF_SSSP);
     k_sssp<<<eng->sssp_blocks, 256, 0, st>>>(g->d_ctx, nctx, G, split);
     prof_end(eng, pe);
-    k_ctrl<<<1, MAXB, 0, st>>>(g->d_ctx, nctx, CTRL_SSSP);
+    k_ctrl<<<nctx, 128, 0, st>>>(g->d_ctx, nctx, CTRL_SSSP);
     eng->cs.launches += 2;
   }
   const size_t per_warp = rows_smem_per_warp(sh.rw_max);
@@ -264,11 +279,11 @@ gst_status launch_level(gst_engine* eng, gst_graph* g, int nctx, const LoopShape
   k_rows<<<eng->grow_blocks, warps * 32, per_warp * warps, st>>>(g->d_ctx, nctx, G, split,
                                                                   sh.rw_max);
   prof_end(eng, pe);
-  k_ctrl<<<1, MAXB, 0, st>>>(g->d_ctx, nctx, CTRL_DP_ROWS);
+  k_ctrl<<<nctx, 128, 0, st>>>(g->d_ctx, nctx, CTRL_DP_ROWS);
   pe = prof_begin(eng, PROF_GROW);
   k_grow<<<eng->grow_blocks, 256, 0, st>>>(g->d_ctx, nctx, G, split);
   prof_end(eng, pe);
-  k_ctrl<<<1, MAXB, 0, st>>>(g->d_ctx, nctx, CTRL_DP_GROW);
+  k_ctrl<<<nctx, 128, 0, st>>>(g->d_ctx, nctx, CTRL_DP_GROW);
   eng->cs.launches += 4;
   CK(cudaGetLastError());
   return GST_OK;
@@ -408,20 +423,42 @@ static gst_status graph_create_impl(gst_engine* eng, int64_t V, int64_t E, const
   if (V < 1 || V >= (int64_t)1 << 27 || E < 0 || !beg || (E > 0 && (!adj || !wt)))
     return fail(eng, GST_BAD_INPUT, "graph: need 1 <= V < 2^27, E >= 0 and non-null arrays");
   if (beg[0] != 0 || beg[V] != E) return fail(eng, GST_BAD_INPUT, "graph: beg_pos[0] must be 0 and beg_pos[V] == E");
-  std::vector<int2> edges((size_t)E);
-  for (int64_t v = 0; v < V; v++) {
+  for (int64_t v = 0; v < V; v++)
     if (beg[v + 1] < beg[v]) return fail(eng, GST_BAD_INPUT, "graph: beg_pos not monotone");
+  // Two device copies of the adjacency: sorted by neighbour (edge-weight lookups
+  // of the tree walk) and sorted by weight, with per vertex the number of edges of
+  // weight <= 2^j (j < WIDX), so that a grow step reads only the edges light enough
+  // to keep its target under the upper bound.
+  std::vector<int2> edges((size_t)E), wedges((size_t)E);
+  std::vector<uint32_t> widx((size_t)V * WIDX);
+  int bad = 0;
+#pragma omp parallel
+  {
     std::vector<std::pair<int32_t, int32_t>> tmp;
-    tmp.reserve((size_t)(beg[v + 1] - beg[v]));
-    for (int64_t i = beg[v]; i < beg[v + 1]; i++) {
-      if (adj[i] < 0 || adj[i] >= V) return fail(eng, GST_BAD_INPUT, "graph: neighbour id out of range");
-      if (wt[i] < 1 || wt[i] > (1 << 24))
-        return fail(eng, GST_BAD_INPUT, "graph: weights must be in [1, 2^24]");
-      tmp.push_back({adj[i], wt[i]});
+#pragma omp for schedule(dynamic, 1024) reduction(| : bad)
+    for (int64_t v = 0; v < V; v++) {
+      tmp.clear();
+      for (int64_t i = beg[v]; i < beg[v + 1]; i++) {
+        if (adj[i] < 0 || adj[i] >= V) bad |= 1;
+        else if (wt[i] < 1 || wt[i] > (1 << 24)) bad |= 2;
+        else tmp.push_back({adj[i], wt[i]});
+      }
+      if (!std::is_sorted(tmp.begin(), tmp.end())) std::sort(tmp.begin(), tmp.end());
+      for (size_t j = 0; j < tmp.size(); j++)
+        edges[beg[v] + j] = make_int2(tmp[j].first, tmp[j].second);
+      for (auto& x : tmp) std::swap(x.first, x.second);
+      std::sort(tmp.begin(), tmp.end());
+      size_t j = 0;
+      for (int t = 0; t < WIDX; t++) {
+        while (j < tmp.size() && tmp[j].first <= (1 << t)) j++;
+        widx[(size_t)v * WIDX + t] = (uint32_t)j;
+      }
+      for (size_t i = 0; i < tmp.size(); i++)
+        wedges[beg[v] + i] = make_int2(tmp[i].second, tmp[i].first);
     }
-    if (!std::is_sorted(tmp.begin(), tmp.end())) std::sort(tmp.begin(), tmp.end());
-    for (size_t j = 0; j < tmp.size(); j++) edges[beg[v] + j] = make_int2(tmp[j].first, tmp[j].second);
   }
+  if (bad & 1) return fail(eng, GST_BAD_INPUT, "graph: neighbour id out of range");
+  if (bad & 2) return fail(eng, GST_BAD_INPUT, "graph: weights must be in [1, 2^24]");
   std::lock_guard<std::mutex> lk(eng->mu);
   CK(cudaSetDevice(eng->device));
   gst_graph* g = new gst_graph();
@@ -431,15 +468,22 @@ static gst_status graph_create_impl(gst_engine* eng, int64_t V, int64_t E, const
   g->h_beg.assign(beg, beg + V + 1);
   CK(cudaMalloc(&g->d_beg, sizeof(int64_t) * (V + 1)));
   CK(cudaMalloc(&g->d_edges, sizeof(int2) * std::max<int64_t>(E, 1)));
+  CK(cudaMalloc(&g->d_wedges, sizeof(int2) * std::max<int64_t>(E, 1)));
+  CK(cudaMalloc(&g->d_widx, sizeof(uint32_t) * V * WIDX));
   CK(cudaMalloc(&g->d_ctx, sizeof(Ctx) * MAXB));
   CK(cudaMallocHost(&g->h_ctx, sizeof(Ctx) * MAXB));
   // stream-ordered copies, completed before returning: the level kernels run on a
   // non-blocking stream that does not wait for the legacy default stream
   CK(cudaMemcpyAsync(g->d_beg, beg, sizeof(int64_t) * (V + 1), cudaMemcpyHostToDevice,
                      eng->stream));
-  if (E)
+  if (E) {
     CK(cudaMemcpyAsync(g->d_edges, edges.data(), sizeof(int2) * E, cudaMemcpyHostToDevice,
                        eng->stream));
+    CK(cudaMemcpyAsync(g->d_wedges, wedges.data(), sizeof(int2) * E, cudaMemcpyHostToDevice,
+                       eng->stream));
+  }
+  CK(cudaMemcpyAsync(g->d_widx, widx.data(), sizeof(uint32_t) * V * WIDX,
+                     cudaMemcpyHostToDevice, eng->stream));
   CK(cudaStreamSynchronize(eng->stream));
   *out = g;
   return GST_OK;
@@ -473,6 +517,8 @@ gst_status gst_graph_destroy(gst_graph* g) {
   for (auto& s : g->slots) free_slot(s);
   cudaFree(g->d_beg);
   cudaFree(g->d_edges);
+  cudaFree(g->d_wedges);
+  cudaFree(g->d_widx);
   cudaFree(g->d_ctx);
   cudaFreeHost(g->h_ctx);
   delete g;
@@ -587,7 +633,7 @@ gst_status gst_solve_batch(gst_graph* g, gst_groups* grp, int32_t n, const gst_q
       eng->cs.h2d += sizeof(Ctx);
       eng->cs.launches += 2;
       // k_init for this slot alone: grid.y selects the context
-      DevGraph G{g->V, g->E, g->d_beg, g->d_edges};
+      const DevGraph G = dev_graph(g);
       k_init<<<dim3(64, 1), 256, 0, eng->stream>>>(g->d_ctx + s, 1, G, grp->d_ptr, grp->d_mem,
                                                    eng->cfg.split_degree);
       k_ctrl<<<1, 32, 0, eng->stream>>>(g->d_ctx + s, 1, CTRL_SSSP);
@@ -623,13 +669,13 @@ gst_status gst_solve_batch(gst_graph* g, gst_groups* grp, int32_t n, const gst_q
       bool any_sssp = false;
       for (int s = 0; s < nslots; s++) {
         if (owner[s] < 0) continue;
-        any_sssp |= g->h_ctx[s].phase == PH_SSSP;
+        any_sssp |= g->h_ctx[s].phase == PH_SSSP || g->h_ctx[s].phase == PH_PREP;
         any_done |= g->h_ctx[s].phase >= PH_DONE;
       }
       sh.sssp = any_sssp;
     }
     // harvest finished queries
-    DevGraph G{g->V, g->E, g->d_beg, g->d_edges};
+    const DevGraph G = dev_graph(g);
     k_extract<<<1, MAXB, 0, eng->stream>>>(g->d_ctx, nslots, G);
     eng->cs.launches += 1;
     CK(cudaMemcpyAsync(g->h_ctx, g->d_ctx, sizeof(Ctx) * nslots, cudaMemcpyDeviceToHost,
@@ -835,6 +881,8 @@ gst_status noalloc_solve(int device, cudaStream_t st, int64_t V, int64_t E, cons
   off = align256(off + (size_t)outcap * 12);
   const size_t o_stack = off;
   off = align256(off + (size_t)stackcap * 8);
+  const size_t o_tour = off;
+  off = align256(off + kTourWords * 4);
   const size_t min_lists = 4 * (size_t)(4 * V + 4096) * 16;
   if (off + min_lists > kNoallocScratchBytes) {
     char msg[200];
@@ -881,6 +929,7 @@ gst_status noalloc_solve(int device, cudaStream_t st, int64_t V, int64_t E, cons
   c.table = (uint64_t*)(base + o_table);
   c.dist = (uint32_t*)(base + o_dist);
   c.rowbits = (uint32_t*)(base + o_bits);
+  c.tour = (uint32_t*)(base + o_tour);
   c.q[0] = (uint4*)(base + off);
   c.q[1] = (uint4*)(base + off + (size_t)cap * 16);
   c.far[0] = (uint4*)(base + off + 2 * (size_t)cap * 16);
@@ -900,7 +949,9 @@ gst_status noalloc_solve(int device, cudaStream_t st, int64_t V, int64_t E, cons
   c.RW = c.W * c.DD;
   c.hop = hop;
   c.use_lb = hop ? 0 : 1;
+  c.use_tour = c.use_lb;
   for (int i = 0; i < q->k; i++) c.gid[i] = q->group_ids[i];
+  memset(c.vv, 0xFF, sizeof(c.vv));
   c.delta = 0;
   c.max_levels = (uint32_t)cfg.max_levels;
   c.in_idx = 1;
@@ -916,7 +967,8 @@ gst_status noalloc_solve(int device, cudaStream_t st, int64_t V, int64_t E, cons
   CK(cudaMemsetAsync(c.dist, 0xFF, (size_t)V * DIST_STRIDE * 4, st));
   CK(cudaMemsetAsync(c.rowbits, 0, ((size_t)V + 31) / 32 * 4, st));
   CK(cudaMemcpyAsync(d_ctx, &c, sizeof(Ctx), cudaMemcpyHostToDevice, st));
-  DevGraph G{V, E, d_beg, (const int2*)d_edges};
+  // the caller's edges are sorted by neighbour only: no light-edge index
+  DevGraph G{V, E, d_beg, (const int2*)d_edges, (const int2*)d_edges, nullptr};
   k_init<<<dim3(64, 1), 256, 0, st>>>(d_ctx, 1, G, d_grp_ptr, d_members, split);
   k_ctrl<<<1, 32, 0, st>>>(d_ctx, 1, CTRL_SSSP);
   const int blocks = sms * cfg.blocks_per_sm;
