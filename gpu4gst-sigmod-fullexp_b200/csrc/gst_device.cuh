@@ -1,8 +1,8 @@
 // Device side of the GST engine: state layout, worklists and the level kernels.
 //
 // State table.  One query owns a slab of V rows; row v holds the 2^k x (D+1)
-// states (v, p, d) of that vertex (d only for hop-bounded queries) as packed
-// 64-bit cells
+// states (v, p, d) of that vertex (d only for hop-bounded queries), cell d * 2^k + p,
+// as packed 64-bit cells
 //     cost(32) | pending(1) | parent(31)
 // so that one 64-bit atomicMin relaxes cost and parent together (the reference
 // writes its int32 cost with atomicMin and the parent separately,
@@ -57,7 +57,13 @@ enum ErrBits : uint32_t { ERR_QCAP = 1, ERR_FARCAP = 2, ERR_ROWCAP = 4, ERR_TIME
                           ERR_EXTRACT = 16, ERR_BOUNDS = 32 };
 enum CtrlMode : int { CTRL_SSSP = 0, CTRL_DP_ROWS = 1, CTRL_DP_GROW = 2 };
 
-constexpr int WIDX = 8;            // light-edge index: counts of edges with w <= 2^j, j < 8
+// Light-edge index: per vertex, the number of edges of weight <= widx_threshold(t)
+// for t < WIDX, thresholds 1, 2, 3, 4, 6, 8, 12, ..., 192, 256 (each step x1.5 or
+// x1.33), so that one load bounds the edges a relaxation under a weight limit
+// needs, over-counting by at most a third.
+constexpr int WIDX = 16;
+constexpr uint32_t CHUNK = 0x80000000u;  // item flag (in pd): one `split`-edge chunk only
+constexpr int RELAX_U = 4;               // edges per lane per round of the relax loops
 constexpr int TOUR_STRIDE = KMAX * KMAX;
 
 struct DevGraph {
@@ -70,14 +76,27 @@ struct DevGraph {
                           // wedges then need not be weight-sorted)
 };
 
-// Number of leading entries of v's weight-sorted edge list that can hold an edge
-// of weight <= lim (an over-count by at most the edges in (lim, 2^j]).
-__device__ __forceinline__ int64_t light_count(const DevGraph& G, uint32_t v, int64_t deg,
-                                               uint32_t lim) {
-  if (lim == 0u) return 0;
-  if (!G.widx || lim > (1u << (WIDX - 1))) return deg;
-  const int j = 32 - __clz(lim - 1u);  // smallest j with 2^j >= lim
-  return (int64_t)__ldg(&G.widx[(uint64_t)v * WIDX + j]);
+__host__ __device__ __forceinline__ uint32_t widx_threshold(int t) {
+  return t == 0 ? 1u : ((t & 1) ? (2u << (t >> 1)) : (3u << ((t >> 1) - 1)));
+}
+// Smallest t with widx_threshold(t) >= W (W >= 1); WIDX when W > 256.
+__device__ __forceinline__ int widx_slot(uint32_t W) {
+  if (W <= 1u) return 0;
+  const int b = 31 - __clz(W - 1u);  // 2^b < W <= 2^(b+1)
+  if (b == 0) return 1;
+  if (b >= 8) return WIDX;
+  return W <= (3u << (b - 1)) ? 2 * b : 2 * b + 1;
+}
+
+// Edges of v (weight-sorted list, deg entries) worth relaxing under the weight limit
+// W: every edge of weight <= W, plus possibly some heavier ones (the per-edge tests
+// drop those).  Without an index the list is not weight-sorted and every edge counts.
+__device__ __forceinline__ int64_t count_upto(const DevGraph& G, uint32_t v, int64_t deg,
+                                              uint32_t W) {
+  if (deg <= 0 || W == 0u) return 0;
+  if (!G.widx) return deg;
+  const int t = widx_slot(W);
+  return t >= WIDX ? deg : (int64_t)__ldg(&G.widx[(uint64_t)v * WIDX + t]);
 }
 
 // Per-query context.  Fields above `in_ptr` are written by the host before the
@@ -113,6 +132,8 @@ struct Ctx {
   uint32_t far_min;
   uint32_t bucket_end;
   uint32_t ub;          // best feasible cost known (one-label solutions and full cells)
+  uint32_t cut;         // ub when the one-label distances became final: a distance above
+                        // it (or unreached) is only known to exceed it
   uint32_t ub_cell;     // best full-state cell
   unsigned long long best;  // cost<<32 | d<<27 | v of the best full-state cell
   uint32_t phase;
@@ -121,6 +142,8 @@ struct Ctx {
   uint32_t n_out;
   uint32_t bad_site;    // checked builds: first failed bounds check (site id)
   unsigned long long st_items, st_relax, st_merge, st_rows, st_sssp;
+  uint32_t st_qmax;     // largest worklist fill seen (near or far), for capacity sizing
+  uint32_t idle;        // 1: no query in this slot (the kernels skip it)
 };
 
 // Bounds self-check of the checked build (-DGST_CHECKED): a failed check records
@@ -154,6 +177,15 @@ __device__ __forceinline__ uint32_t deposit(uint32_t b, uint32_t mask) {
   return r;
 }
 
+// x / y for x < 2^22 and 1 <= y, from a float estimate and one correction each way
+// (inv = 1.0f / y computed once by the caller).
+__device__ __forceinline__ uint32_t udiv_small(uint32_t x, uint32_t y, float inv) {
+  uint32_t q = (uint32_t)((float)x * inv);
+  if (q * y > x) q--;
+  if ((q + 1u) * y <= x) q++;
+  return q;
+}
+
 // First lane whose inclusive scan value exceeds i (all lanes participate).
 __device__ __forceinline__ int warp_owner(uint32_t scan, uint32_t i) {
   int lo = 0;
@@ -175,30 +207,15 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x) {
   return x;
 }
 
-// ---- worklist pushes ---------------------------------------------------------
-__device__ __forceinline__ void push_near(Ctx* c, const uint4& e) {
-  const uint32_t i = atomicAdd(&c->n_q[c->no], 1u);
-  if (i < c->qcap) c->q[c->no][i] = e;
-  else atomicOr(&c->error, (uint32_t)ERR_QCAP);
-}
-__device__ __forceinline__ void push_far(Ctx* c, const uint4& e) {
-  const uint32_t i = atomicAdd(&c->n_far[c->f], 1u);
-  if (i < c->farcap) c->far[c->f][i] = e;
-  else atomicOr(&c->error, (uint32_t)ERR_FARCAP);
-  atomicMin(&c->far_min, e.z);
-}
-// Emit the work items of state (v, pd) with cost `cost`: one per `split` edges of
-// the first `cnt` entries of v's edge list.
-__device__ __forceinline__ void push_state(Ctx* c, uint32_t v, uint32_t pd, uint32_t cost,
-                                           int64_t cnt, int split, uint32_t bucket_end) {
-  const uint32_t nch = (uint32_t)((cnt + split - 1) / split);
-  const bool near = cost < bucket_end;
-  for (uint32_t ch = 0; ch < nch; ch++) {
-    const uint4 e = make_uint4(v, pd, cost, ch);
-    if (near) push_near(c, e);
-    else push_far(c, e);
-  }
-}
+// ---- worklists -----------------------------------------------------------------
+// A work item {v, pd, cost, off} asks for the edges of v's weight-sorted list from
+// offset `off` on to be relaxed from state (v, pd) of cost `cost` (pd: group index
+// in the distance phase, subset | hop << 16 in the DP).  Edges are relaxed in weight
+// order and only as far as the current cost bucket [.., bucket_end) and the upper
+// bound allow; an item whose next edge lands beyond the bucket waits in the far
+// list under the key cost + weight(next edge), so heavy edges are read only once
+// the frontier has reached their target cost, by which time ub has usually pruned
+// them.  The near list holds items of the current bucket.
 // Largest edge weight a grow step from a state of cost `cost` can still use: a
 // target must stay <= ub (unbounded) or < ub_cell (hop-bounded).
 __device__ __forceinline__ uint32_t grow_limit(const Ctx* c, uint32_t cost) {
@@ -220,20 +237,185 @@ __device__ __forceinline__ void mark_row(Ctx* c, uint32_t u) {
   }
 }
 
-// Per-CTA prefix of the input counts of all queries of the launch.
-// want: PH_SSSP (sssp input), PH_DP (grow input) or -1 (rows of DP-phase queries).
-__device__ __forceinline__ void load_prefix(Ctx* ctxs, int nctx, uint32_t* s_pref, int want) {
-  if (threadIdx.x == 0) {
-    uint32_t acc = 0;
-    s_pref[0] = 0;
-    for (int i = 0; i < nctx; i++) {
-      const Ctx* c = ctxs + i;
-      uint32_t n = 0;
-      if (want < 0) n = (c->phase == PH_DP) ? min(c->n_rows, c->rowcap) : 0u;
-      else n = (c->phase == (uint32_t)want) ? c->in_n : 0u;
-      acc += n;
-      s_pref[i + 1] = acc;
+// ---- warp-aggregated appends (all 32 lanes call; the loops are warp-uniform) ----
+// One worklist counter per query is the hottest address of a level: lanes that
+// append to the same list (same query, near or far) reserve their slots with one
+// atomicAdd per warp, and far appends lower far_min once per warp.
+// Lane with `want` appends item {v, pd, cost, off} to query qi's near list (far ==
+// false) or far list (far == true, under `key`).
+__device__ __forceinline__ void warp_append(Ctx* ctxs, int qi, bool want, bool far, uint32_t v,
+                                            uint32_t pd, uint32_t cost, uint32_t off,
+                                            uint32_t key) {
+  const int lane = threadIdx.x & 31;
+  uint32_t todo = __ballot_sync(0xffffffffu, want);
+  while (todo) {
+    const int leader = __ffs(todo) - 1;
+    const int lq = __shfl_sync(0xffffffffu, qi, leader);
+    const int lf = __shfl_sync(0xffffffffu, (int)far, leader);
+    const bool mine = want && qi == lq && (int)far == lf;
+    const uint32_t grp = __ballot_sync(0xffffffffu, mine);
+    const uint32_t kmin = __reduce_min_sync(0xffffffffu, mine ? key : 0xFFFFFFFFu);
+    Ctx* c = ctxs + lq;
+    uint32_t base = 0;
+    if (lane == leader) {
+      base = atomicAdd(lf ? &c->n_far[c->f] : &c->n_q[c->no], (uint32_t)__popc(grp));
+      if (lf) atomicMin(&c->far_min, kmin);
     }
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (mine) {
+      const uint32_t i = base + __popc(grp & ((1u << lane) - 1u));
+      if (lf) {
+        if (i < c->farcap) c->far[c->f][i] = make_uint4(v, pd, cost, off);
+        else atomicOr(&c->error, (uint32_t)ERR_FARCAP);
+      } else {
+        if (i < c->qcap) c->q[c->no][i] = make_uint4(v, pd, cost, off);
+        else atomicOr(&c->error, (uint32_t)ERR_QCAP);
+      }
+    }
+    todo &= ~grp;
+  }
+}
+
+// Lane appends the n chunk items {v, pd | CHUNK, cost, off + j * split}, j < n, to
+// query qi's near list.
+__device__ __forceinline__ void warp_append_chunks(Ctx* ctxs, int qi, uint32_t n, uint32_t v,
+                                                   uint32_t pd, uint32_t cost, uint32_t off,
+                                                   int split) {
+  const int lane = threadIdx.x & 31;
+  uint32_t todo = __ballot_sync(0xffffffffu, n > 0);
+  while (todo) {
+    const int leader = __ffs(todo) - 1;
+    const int lq = __shfl_sync(0xffffffffu, qi, leader);
+    const bool mine = n > 0 && qi == lq;
+    const uint32_t x = mine ? n : 0u;
+    const uint32_t scan = warp_incl_scan(x);
+    const uint32_t total = __shfl_sync(0xffffffffu, scan, 31);
+    Ctx* c = ctxs + lq;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(&c->n_q[c->no], total);
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (mine) {
+      uint32_t i = base + scan - x;
+      for (uint32_t j = 0; j < n; j++, i++) {
+        if (i < c->qcap) c->q[c->no][i] = make_uint4(v, pd | CHUNK, cost, off + j * (uint32_t)split);
+        else atomicOr(&c->error, (uint32_t)ERR_QCAP);
+      }
+    }
+    todo &= ~__ballot_sync(0xffffffffu, mine);
+  }
+}
+
+// Plan the item {v, pd, cost, off}: the edge range [eb, eb + n) to relax now, and at
+// most one follow-up item (a continuation of a long range into the near list, or
+// the rest of the list into the far list under the key of its next edge).
+// wmax: heaviest edge the state may still use (the upper bound's limit).
+// A head item (no CHUNK flag) relaxes the first `split` edges of its range now and
+// spawns chunk items for the rest of the range, which the next step relaxes in
+// parallel (hub vertices spread over many warps); only a head item defers the
+// remainder of its list to the far list.  A chunk item relaxes its chunk only.
+struct Plan {
+  int64_t eb;
+  uint32_t n;
+  bool push, far;
+  uint32_t off, key;
+  uint32_t spawn;   // chunk items to append at offsets off + n + j * split
+};
+__device__ __forceinline__ Plan plan_item(const DevGraph& G, uint32_t v, uint32_t cost, uint32_t off,
+                                          uint32_t wmax, uint32_t bucket_end, int split,
+                                          bool chunk) {
+  Plan P{0, 0u, false, false, 0u, 0u, 0u};
+  // the loads below depend only on the item, so they are issued together
+  const int64_t b0 = G.beg[v], b1 = G.beg[v + 1];
+  const int64_t deg = b1 - b0;
+  const uint64_t in_bucket = bucket_end > cost ? (uint64_t)bucket_end - cost - 1u : 0u;
+  const uint32_t hw = (uint32_t)min((uint64_t)wmax, in_bucket);
+  const int64_t cnt = count_upto(G, v, deg, hw);
+  if ((int64_t)off >= deg) return P;
+  if (chunk) {  // a chunk of a range planned by its head item
+    const int64_t end = min(cnt, (int64_t)off + split);
+    if (end > (int64_t)off) {
+      P.eb = b0 + off;
+      P.n = (uint32_t)(end - off);
+    }
+    return P;
+  }
+  if (cnt <= (int64_t)off) {
+    // nothing of this bucket left: defer to the bucket of the next edge, if the
+    // bound still allows it
+    if (!G.widx) return P;
+    const uint32_t w0 = (uint32_t)__ldg(&G.wedges[b0 + off].y);
+    if (w0 > wmax) return P;
+    P.push = P.far = true;
+    P.off = off;
+    P.key = (uint32_t)min((uint64_t)cost + w0, (uint64_t)0xFFFFFFFEu);
+    return P;
+  }
+  const int64_t end = cnt;
+  const int64_t stop = min(end, (int64_t)off + split);
+  P.eb = b0 + off;
+  P.n = (uint32_t)(stop - off);
+  if (stop < end) P.spawn = (uint32_t)((end - stop + split - 1) / split);
+  if (end < deg && hw < wmax) {
+    // the rest of the list waits for the bucket of its first edge
+    const uint32_t w1 = (uint32_t)__ldg(&G.wedges[b0 + end].y);
+    if (w1 <= wmax) {
+      P.push = P.far = true;
+      P.off = (uint32_t)end;
+      P.key = (uint32_t)min((uint64_t)cost + max(w1, hw + 1u), (uint64_t)0xFFFFFFFEu);
+    }
+  }
+  return P;
+}
+
+// Lane with `want` marks row u of query qi dirty; rows newly marked are appended
+// to the query's row list with one atomicAdd per warp and query.
+__device__ __forceinline__ void warp_mark_row(Ctx* ctxs, int qi, bool want, uint32_t u) {
+  const int lane = threadIdx.x & 31;
+  bool fresh = false;
+  if (want) {
+    Ctx* c = ctxs + qi;
+    const uint32_t bit = 1u << (u & 31);
+    fresh = !(atomicOr(&c->rowbits[u >> 5], bit) & bit);
+  }
+  uint32_t todo = __ballot_sync(0xffffffffu, fresh);
+  while (todo) {
+    const int leader = __ffs(todo) - 1;
+    const int lq = __shfl_sync(0xffffffffu, qi, leader);
+    const bool mine = fresh && qi == lq;
+    const uint32_t grp = __ballot_sync(0xffffffffu, mine);
+    Ctx* c = ctxs + lq;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(&c->n_rows, (uint32_t)__popc(grp));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (mine) {
+      const uint32_t i = base + __popc(grp & ((1u << lane) - 1u));
+      if (i < c->rowcap) c->rows[i] = u;
+      else atomicOr(&c->error, (uint32_t)ERR_ROWCAP);
+    }
+    todo &= ~grp;
+  }
+}
+
+
+// Per-CTA prefix of the input counts of all queries of the launch (MAXB <= 64:
+// the first warp loads two contexts per lane and scans them).
+// want: PH_SSSP (sssp input), PH_DP (grow input) or -1 (rows of DP-phase queries).
+__device__ __forceinline__ uint32_t ctx_count(const Ctx* c, int want) {
+  if (want < 0) return (c->phase == PH_DP) ? min(c->n_rows, c->rowcap) : 0u;
+  return (c->phase == (uint32_t)want) ? c->in_n : 0u;
+}
+__device__ __forceinline__ void load_prefix(Ctx* ctxs, int nctx, uint32_t* s_pref, int want) {
+  static_assert(MAXB <= 64, "load_prefix scans two contexts per lane");
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    const uint32_t n0 = lane < nctx ? ctx_count(ctxs + lane, want) : 0u;
+    const uint32_t n1 = lane + 32 < nctx ? ctx_count(ctxs + lane + 32, want) : 0u;
+    const uint32_t s0 = warp_incl_scan(n0);
+    const uint32_t t0 = __shfl_sync(0xffffffffu, s0, 31);
+    const uint32_t s1 = warp_incl_scan(n1) + t0;
+    if (lane == 0) s_pref[0] = 0;
+    if (lane < nctx) s_pref[lane + 1] = s0;
+    if (lane + 32 < nctx) s_pref[lane + 33] = s1;
   }
   __syncthreads();
 }
@@ -273,14 +455,15 @@ __global__ void k_init(Ctx* ctxs, int nctx, DevGraph G, const int64_t* grp_ptr,
         const uint32_t v = (uint32_t)members[j];
         if (!in_bounds(c, v < G.V && i < c->k, 1)) continue;
         const uint64_t cell0 = pack_cell(0, PEND | LEAF);
-        atomicMin((unsigned long long*)&c->table[(uint64_t)v * c->RW + (uint64_t)(1u << i) * c->DD],
+        atomicMin((unsigned long long*)&c->table[(uint64_t)v * c->RW + (1u << i)],
                   (unsigned long long)cell0);
         mark_row(c, v);
         if (c->phase == PH_SSSP) {
           const uint32_t old = atomicMin(&c->dist[(uint64_t)v * DIST_STRIDE + i], 0u);
-          if (old != 0u) {
-            const int64_t deg = G.beg[v + 1] - G.beg[v];
-            push_state(c, v, (uint32_t)i, 0u, deg, split, 0xFFFFFFFFu);
+          if (old != 0u && G.beg[v + 1] > G.beg[v]) {
+            const uint32_t n = atomicAdd(&c->n_q[c->no], 1u);
+            if (n < c->qcap) c->q[c->no][n] = make_uint4(v, (uint32_t)i, 0u, 0u);
+            else atomicOr(&c->error, (uint32_t)ERR_QCAP);
           }
         }
       }
@@ -301,9 +484,9 @@ __global__ void __launch_bounds__(256) k_sssp(Ctx* ctxs, int nctx, DevGraph G, i
   const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   for (uint32_t base = wid * 32; base < total; base += warps * 32) {
     const uint32_t it = base + lane;
-    uint32_t n = 0, v = 0, gi = 0, cost = 0;
-    int64_t eb = 0;
+    uint32_t v = 0, gi = 0, cost = 0, ub = 0, bend = 0, e_off = 0;
     int qi = 0;
+    Plan P{0, 0u, false, false, 0u, 0u, 0u};
     if (it < total) {
       qi = find_ctx(s_pref, nctx, it);
       Ctx* c = ctxs + qi;
@@ -311,47 +494,84 @@ __global__ void __launch_bounds__(256) k_sssp(Ctx* ctxs, int nctx, DevGraph G, i
       v = e.x;
       gi = e.y;
       cost = e.z;
-      if (!in_bounds(c, v < G.V && gi < (uint32_t)c->k, 2)) { v = 0; gi = 0; cost = 0xFFFFFFFFu; }
-      const uint32_t cur = __ldcg(&c->dist[(uint64_t)v * DIST_STRIDE + gi]);
-      if (cur >= cost) {  // not stale
-        if (cost >= c->bucket_end) {
-          push_far(c, e);
-        } else {
-          const int64_t b0 = G.beg[v], b1 = G.beg[v + 1];
-          eb = b0 + (int64_t)e.w * split;
-          const int64_t ee = min(b1, eb + (int64_t)split);
-          n = ee > eb ? (uint32_t)(ee - eb) : 0u;
-        }
+      e_off = e.w;
+      if (in_bounds(c, v < G.V && (gi & ~CHUNK) < (uint32_t)c->k, 2)) {
+        const uint32_t cur = __ldcg(&c->dist[(uint64_t)v * DIST_STRIDE + (gi & ~CHUNK)]);
+        // ub is read once per item (a per-edge read of one word by every thread of
+        // a one-query launch is an L2 hot spot); a stale, larger ub prunes less
+        ub = __ldcg(&c->ub);
+        bend = c->bucket_end;
+        // not stale, and still able to reach a vertex at distance <= ub
+        if (cur >= cost && cost < ub)
+          P = plan_item(G, v, cost, e.w, ub - cost, bend, split, (gi & CHUNK) != 0u);
       }
+      gi &= ~CHUNK;
     }
+    warp_append(ctxs, qi, P.push, P.far, v, gi, cost, P.off, P.key);
+    warp_append_chunks(ctxs, qi, P.spawn, v, gi, cost, e_off + P.n, split);
+    const uint32_t n = P.n;
+    const int64_t eb = P.eb;
     add_stat(ctxs, qi, it < total, n, &Ctx::st_sssp);
     const uint32_t scan = warp_incl_scan(n);
     const uint32_t tot = __shfl_sync(0xffffffffu, scan, 31);
-    for (uint32_t j0 = 0; j0 < tot; j0 += 32) {
-      const uint32_t j = j0 + lane;
-      const int o = warp_owner(scan, j < tot ? j : tot - 1);
-      const uint32_t o_scan = __shfl_sync(0xffffffffu, scan, o);
-      const uint32_t o_n = __shfl_sync(0xffffffffu, n, o);
-      const int64_t o_eb = __shfl_sync(0xffffffffu, eb, o);
-      const uint32_t o_gi = __shfl_sync(0xffffffffu, gi, o);
-      const uint32_t o_cost = __shfl_sync(0xffffffffu, cost, o);
-      const int o_qi = __shfl_sync(0xffffffffu, qi, o);
-      if (j < tot) {
+    // RELAX_U edges per lane per round: their loads are independent, so a warp has
+    // RELAX_U edge loads, then RELAX_U distance loads, in flight at once
+    for (uint32_t j0 = 0; j0 < tot; j0 += 32 * RELAX_U) {
+      int2 ed[RELAX_U];
+      uint32_t x_gi[RELAX_U], x_cost[RELAX_U], x_ub[RELAX_U], x_bend[RELAX_U], cur[RELAX_U];
+      int x_qi[RELAX_U];
+      bool ok[RELAX_U];
+#pragma unroll
+      for (int x = 0; x < RELAX_U; x++) {
+        const uint32_t j = j0 + (uint32_t)x * 32u + lane;
+        const int o = warp_owner(scan, j < tot ? j : tot - 1);
+        const uint32_t o_scan = __shfl_sync(0xffffffffu, scan, o);
+        const uint32_t o_n = __shfl_sync(0xffffffffu, n, o);
+        const int64_t o_eb = __shfl_sync(0xffffffffu, eb, o);
+        x_gi[x] = __shfl_sync(0xffffffffu, gi, o);
+        x_cost[x] = __shfl_sync(0xffffffffu, cost, o);
+        x_ub[x] = __shfl_sync(0xffffffffu, ub, o);
+        x_bend[x] = __shfl_sync(0xffffffffu, bend, o);
+        x_qi[x] = __shfl_sync(0xffffffffu, qi, o);
         const uint32_t off = j - (o_scan - o_n);
-        Ctx* c = ctxs + o_qi;
-        if (!in_bounds(c, o_eb + off < G.E, 3)) continue;
-        const int2 ed = G.wedges[o_eb + off];
-        const uint32_t u = (uint32_t)ed.x;
-        const uint32_t nd = o_cost + (uint32_t)ed.y;
-        if (!in_bounds(c, u < G.V, 4)) continue;
-        uint32_t* dp = &c->dist[(uint64_t)u * DIST_STRIDE + o_gi];
-        if (nd < __ldcg(dp)) {
-          const uint32_t old = atomicMin(dp, nd);
+        ok[x] = j < tot && in_bounds(ctxs + x_qi[x], o_eb + off < G.E, 3);
+        ed[x] = ok[x] ? G.wedges[o_eb + off] : make_int2(0, 0);
+      }
+#pragma unroll
+      for (int x = 0; x < RELAX_U; x++) {
+        const uint32_t u = (uint32_t)ed[x].x, nd = x_cost[x] + (uint32_t)ed[x].y;
+        // distances above ub are never needed exactly: a state whose missing group
+        // lies further than ub is pruned whatever the exact distance
+        ok[x] = ok[x] && in_bounds(ctxs + x_qi[x], u < G.V, 4) && nd <= x_ub[x];
+        cur[x] = ok[x] ? __ldcg(&ctxs[x_qi[x]].dist[(uint64_t)u * DIST_STRIDE + x_gi[x]]) : 0u;
+      }
+#pragma unroll
+      for (int x = 0; x < RELAX_U; x++) {
+        const uint32_t u = (uint32_t)ed[x].x, nd = x_cost[x] + (uint32_t)ed[x].y;
+        Ctx* c = ctxs + x_qi[x];
+        bool push = false;
+        if (ok[x] && nd < cur[x]) {
+          const uint32_t old = atomicMin(&c->dist[(uint64_t)u * DIST_STRIDE + x_gi[x]], nd);
           if (nd < old) {
-            const int64_t deg = G.beg[u + 1] - G.beg[u];
-            push_state(c, u, o_gi, nd, deg, split, c->bucket_end);
+            // star bound from tentative distances: the k paths found so far from u
+            // to a member of each group form a connected subgraph covering every
+            // group, so their total length is a feasible cost
+            const uint4* row = (const uint4*)&c->dist[(uint64_t)u * DIST_STRIDE];
+            const uint4 a = __ldcg(row), b = __ldcg(row + 1);
+            const uint32_t d[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+            const int k = c->k;
+            uint64_t sum = 0;
+#pragma unroll
+            for (int i = 0; i < KMAX; i++)
+              if (i < k) sum += (i == (int)x_gi[x]) ? nd : d[i];
+            if (sum < (uint64_t)x_ub[x]) atomicMin(&c->ub, (uint32_t)sum);
+            push = nd < x_ub[x];
           }
         }
+        // an improved vertex relaxes its own edges from the lightest one, which lands
+        // at nd + 1 or later: in this bucket or a later one
+        const bool far = (uint64_t)nd + 1u >= x_bend[x];
+        warp_append(ctxs, x_qi[x], push, far, u, x_gi[x], nd, 0u, nd + 1u);
       }
     }
   }
@@ -399,80 +619,102 @@ __global__ void __launch_bounds__(256) k_grow(Ctx* ctxs, int nctx, DevGraph G, i
   const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   for (uint32_t base = wid * 32; base < total; base += warps * 32) {
     const uint32_t it = base + lane;
-    uint32_t n = 0, v = 0, pd = 0, cost = 0;
-    int64_t eb = 0;
+    uint32_t v = 0, pd = 0, cost = 0, bound = 0, e_off = 0;
+    bool chunk = false;
     int qi = 0;
+    Plan P{0, 0u, false, false, 0u, 0u, 0u};
     if (it < total) {
       qi = find_ctx(s_pref, nctx, it);
       Ctx* c = ctxs + qi;
       const uint4 e = c->in_ptr[it - s_pref[qi]];
       v = e.x;
-      pd = e.y;
+      chunk = (e.y & CHUNK) != 0u;
+      pd = e.y & ~CHUNK;
       cost = e.z;
+      e_off = e.w;
       const uint32_t p = pd & 0xFFFFu, d = pd >> 16;
       const bool ok = in_bounds(c, v < G.V && p < (uint32_t)c->W && d < (uint32_t)c->DD, 5);
       const uint64_t cell = ok ? __ldcg((const unsigned long long*)&c->table[(uint64_t)v * c->RW +
-                                                                           (uint64_t)p * c->DD + d])
+                                                                           ((uint64_t)d << c->k) + p])
                                : 0ull;
-      const uint32_t bound = c->hop ? c->ub_cell : c->ub;
+      bound = c->hop ? __ldcg(&c->ub_cell) : __ldcg(&c->ub);
       // a work item always names a state that holds a finite cost
       const bool src_ok = !ok || in_bounds(c, cost_of(cell) != COST_INF, 12);
       if (ok && src_ok && cost_of(cell) >= cost && 2ull * cost <= (uint64_t)bound) {
-        if (cost >= c->bucket_end) {
-          push_far(c, e);
-        } else {
-          const int64_t b0 = G.beg[v], b1 = G.beg[v + 1];
-          const int64_t lc = light_count(G, v, b1 - b0, grow_limit(c, cost));
-          eb = b0 + (int64_t)e.w * split;
-          const int64_t ee = min(b0 + lc, eb + (int64_t)split);
-          n = ee > eb ? (uint32_t)(ee - eb) : 0u;
-        }
+        const uint32_t wmax = c->hop ? (bound > cost ? bound - cost - 1u : 0u)
+                                     : (bound >= cost ? bound - cost : 0u);
+        P = plan_item(G, v, cost, e.w, wmax, c->bucket_end, split, chunk);
       }
     }
+    warp_append(ctxs, qi, P.push, P.far, v, pd, cost, P.off, P.key);
+    warp_append_chunks(ctxs, qi, P.spawn, v, pd, cost, e_off + P.n, split);
+    const uint32_t n = P.n;
+    const int64_t eb = P.eb;
     add_stat(ctxs, qi, it < total, n, &Ctx::st_relax);
     add_stat(ctxs, qi, it < total, n > 0 ? 1u : 0u, &Ctx::st_items);
     const uint32_t scan = warp_incl_scan(n);
     const uint32_t tot = __shfl_sync(0xffffffffu, scan, 31);
-    for (uint32_t j0 = 0; j0 < tot; j0 += 32) {
-      const uint32_t j = j0 + lane;
-      const int o = warp_owner(scan, j < tot ? j : tot - 1);
-      const uint32_t o_scan = __shfl_sync(0xffffffffu, scan, o);
-      const uint32_t o_n = __shfl_sync(0xffffffffu, n, o);
-      const int64_t o_eb = __shfl_sync(0xffffffffu, eb, o);
-      const uint32_t o_v = __shfl_sync(0xffffffffu, v, o);
-      const uint32_t o_pd = __shfl_sync(0xffffffffu, pd, o);
-      const uint32_t o_cost = __shfl_sync(0xffffffffu, cost, o);
-      const int o_qi = __shfl_sync(0xffffffffu, qi, o);
-      if (j < tot) {
-        Ctx* c = ctxs + o_qi;
+    for (uint32_t j0 = 0; j0 < tot; j0 += 32 * RELAX_U) {
+      int2 ed[RELAX_U];
+      uint32_t x_v[RELAX_U], x_pd[RELAX_U], x_cost[RELAX_U], x_bound[RELAX_U];
+      uint64_t cur[RELAX_U];
+      int x_qi[RELAX_U];
+      bool ok[RELAX_U];
+#pragma unroll
+      for (int x = 0; x < RELAX_U; x++) {
+        const uint32_t j = j0 + (uint32_t)x * 32u + lane;
+        const int o = warp_owner(scan, j < tot ? j : tot - 1);
+        const uint32_t o_scan = __shfl_sync(0xffffffffu, scan, o);
+        const uint32_t o_n = __shfl_sync(0xffffffffu, n, o);
+        const int64_t o_eb = __shfl_sync(0xffffffffu, eb, o);
+        x_v[x] = __shfl_sync(0xffffffffu, v, o);
+        x_pd[x] = __shfl_sync(0xffffffffu, pd, o);
+        x_cost[x] = __shfl_sync(0xffffffffu, cost, o);
+        x_bound[x] = __shfl_sync(0xffffffffu, bound, o);
+        x_qi[x] = __shfl_sync(0xffffffffu, qi, o);
         const uint32_t off = j - (o_scan - o_n);
-        if (!in_bounds(c, o_eb + off < G.E, 6)) continue;
-        const int2 ed = G.wedges[o_eb + off];
-        const uint32_t u = (uint32_t)ed.x;
-        const uint32_t nc = o_cost + (uint32_t)ed.y;
-        if (!in_bounds(c, u < G.V, 7)) continue;
+        ok[x] = j < tot && in_bounds(ctxs + x_qi[x], o_eb + off < G.E, 6);
+        ed[x] = ok[x] ? G.wedges[o_eb + off] : make_int2(0, 0);
+      }
+#pragma unroll
+      for (int x = 0; x < RELAX_U; x++) {
+        Ctx* c = ctxs + x_qi[x];
+        const uint32_t u = (uint32_t)ed[x].x, nc = x_cost[x] + (uint32_t)ed[x].y;
         // a target costing more than ub cannot be part of an optimal tree
-        const bool keep = c->hop ? (nc < c->ub_cell) : (nc <= c->ub);
-        if (keep) {
-          const uint32_t p = o_pd & 0xFFFFu, d = (o_pd >> 16) + (uint32_t)c->hop;
-          if (!in_bounds(c, d < (uint32_t)c->DD, 11)) continue;
-          unsigned long long* tp =
-              (unsigned long long*)&c->table[(uint64_t)u * c->RW + (uint64_t)p * c->DD + d];
-          const uint64_t nv = pack_cell(nc, PEND | o_v);
-          if (nv < __ldcg(tp)) {
+        const int hop = c->hop;
+        const bool keep = hop ? (nc < x_bound[x]) : (nc <= x_bound[x]);
+        const uint32_t p = x_pd[x] & 0xFFFFu, d = (x_pd[x] >> 16) + (uint32_t)hop;
+        ok[x] = ok[x] && in_bounds(c, u < G.V, 7) && keep && in_bounds(c, d < (uint32_t)c->DD, 11);
+        cur[x] = ok[x] ? __ldcg((const unsigned long long*)&c->table[(uint64_t)u * c->RW +
+                                                                     ((uint64_t)d << c->k) + p])
+                       : 0ull;
+      }
+#pragma unroll
+      for (int x = 0; x < RELAX_U; x++) {
+        Ctx* c = ctxs + x_qi[x];
+        const uint32_t u = (uint32_t)ed[x].x, nc = x_cost[x] + (uint32_t)ed[x].y;
+        bool dirty = false;
+        if (ok[x]) {
+          const uint32_t p = x_pd[x] & 0xFFFFu, d = (x_pd[x] >> 16) + (uint32_t)c->hop;
+          const uint64_t nv = pack_cell(nc, PEND | x_v[x]);
+          if (nv < cur[x]) {
+            unsigned long long* tp =
+                (unsigned long long*)&c->table[(uint64_t)u * c->RW + ((uint64_t)d << c->k) + p];
             const uint64_t old = atomicMin(tp, (unsigned long long)nv);
-            if (cost_of(old) > nc) mark_row(c, u);
+            dirty = cost_of(old) > nc;
           }
         }
+        warp_mark_row(ctxs, x_qi[x], dirty, u);
       }
     }
   }
 }
 
 // ---- DP rows step: merge closure of dirty rows in shared memory -------------------
-// Per-warp shared memory: RW cells, RW/32 pending words, RW list slots (16-B aligned).
+// Per-warp shared memory: RW cells, RW/32 pending words, two lists of RW cell
+// indices (pending operands, finite partners), 16-B aligned.
 __host__ __device__ __forceinline__ size_t rows_smem_per_warp(int rw_max) {
-  const size_t b = (size_t)rw_max * 8 + (size_t)((rw_max + 31) / 32) * 4 + (size_t)rw_max * 2;
+  const size_t b = (size_t)rw_max * 8 + (size_t)((rw_max + 31) / 32) * 4 + (size_t)rw_max * 4;
   return (b + 15) & ~(size_t)15;
 }
 
@@ -480,6 +722,7 @@ __host__ __device__ __forceinline__ size_t rows_smem_per_warp(int rw_max) {
 __global__ void __launch_bounds__(256) k_rows(Ctx* ctxs, int nctx, DevGraph G, int split,
                                               int rw_max) {
   __shared__ uint32_t s_pref[MAXB + 1];
+  __shared__ uint32_t wcls[32];  // per warp: popcount classes holding pending cells
   extern __shared__ __align__(16) unsigned char s_dyn[];
   load_prefix(ctxs, nctx, s_pref, -1);
   const uint32_t total = s_pref[nctx];
@@ -490,18 +733,23 @@ __global__ void __launch_bounds__(256) k_rows(Ctx* ctxs, int nctx, DevGraph G, i
   unsigned long long* buf = (unsigned long long*)wbase;
   uint32_t* pend = (uint32_t*)(wbase + (size_t)rw_max * 8);
   uint16_t* list = (uint16_t*)(wbase + (size_t)rw_max * 8 + (size_t)((rw_max + 31) / 32) * 4);
+  uint16_t* flist = list + rw_max;
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int st_q = -1;
+  unsigned long long st_merges = 0, st_rows = 0;
   for (uint32_t it = wid; it < total; it += warps) {
     uint32_t merges = 0;
     const int qi = find_ctx(s_pref, nctx, it);
     Ctx* c = ctxs + qi;
     const uint32_t v = c->rows[it - s_pref[qi]];
     if (!in_bounds(c, v < G.V && c->RW <= rw_max, 8)) continue;
-    const int RW = c->RW, DD = c->DD, k = c->k, D = c->D, hop = c->hop;
+    const int RW = c->RW, W = c->W, DD = c->DD, k = c->k, D = c->D, hop = c->hop;
+    (void)W;
     const uint32_t full = (uint32_t)c->full;
     unsigned long long* row = (unsigned long long*)&c->table[(uint64_t)v * RW];
-    // load row, collect pending bits
+    // load row, collect pending bits and the popcount classes that hold pending cells
+    uint32_t cls = 0;
     for (int i0 = 0; i0 < RW; i0 += 32) {
       const int i = i0 + lane;
       uint64_t x = CELL_INF;
@@ -510,70 +758,115 @@ __global__ void __launch_bounds__(256) k_rows(Ctx* ctxs, int nctx, DevGraph G, i
         buf[i] = x;
       }
       // an unreached cell is all ones, so its pending bit must be ignored
-      const uint32_t bal =
-          __ballot_sync(0xffffffffu, i < RW && x != CELL_INF && ((uint32_t)x & PEND));
+      const bool pn = i < RW && x != CELL_INF && ((uint32_t)x & PEND);
+      const uint32_t bal = __ballot_sync(0xffffffffu, pn);
+      if (pn) cls |= 1u << __popc((uint32_t)i & full);
       if (lane == 0) pend[i0 >> 5] = bal;
     }
-    if (lane == 0) atomicAnd(&c->rowbits[v >> 5], ~(1u << (v & 31)));
+    cls = __reduce_or_sync(0xffffffffu, cls);
+    if (lane == 0) {
+      wcls[wib] = cls;
+      atomicAnd(&c->rowbits[v >> 5], ~(1u << (v & 31)));
+    }
     __syncwarp();
     const uint32_t ubm = hop ? c->ub_cell : c->ub;
-    // merge closure, by popcount class of the pending operand
+    // merge closure, by popcount class of the pending operand.  A pending cell X of
+    // class j is merged with every finite cell Y disjoint from it: either by
+    // enumerating the submasks of X's complement, or, when the row holds fewer
+    // finite partners than that, by scanning the list of finite cells.
     for (int j = 1; j < k; j++) {
-      int nl = 0;
+      // classes without pending cells are skipped (merges that create or improve a
+      // cell of a higher class record it in wcls)
+      if (!((*(volatile uint32_t*)&wcls[wib] >> j) & 1u)) continue;
+      int nl = 0, nf = 0;
       for (int i0 = 0; i0 < RW; i0 += 32) {
         const int i = i0 + lane;
-        const bool sel = i < RW && ((pend[i >> 5] >> (i & 31)) & 1u) && __popc(i / DD) == j;
+        const uint32_t pc = i < RW ? (uint32_t)__popc((uint32_t)i & full) : 0u;
+        const bool sel = i < RW && ((pend[i >> 5] >> (i & 31)) & 1u) && pc == (uint32_t)j;
+        const bool fin = i < RW && pc >= 1u && pc <= (uint32_t)(k - j) &&
+                         cost_of(buf[i]) != COST_INF;
         const uint32_t bal = __ballot_sync(0xffffffffu, sel);
+        const uint32_t bf = __ballot_sync(0xffffffffu, fin);
         if (sel) list[nl + __popc(bal & ((1u << lane) - 1u))] = (uint16_t)i;
+        if (fin) flist[nf + __popc(bf & ((1u << lane) - 1u))] = (uint16_t)i;
         nl += __popc(bal);
+        nf += __popc(bf);
       }
       __syncwarp();
-      if (nl == 0) continue;
+      if (nl == 0 || nf == 0) continue;
       const uint32_t m = (1u << (k - j)) - 1u;  // non-empty submasks of the complement
-      const uint32_t per = m * (uint32_t)DD;
+      const bool scan_f = (uint32_t)nf < m * (uint32_t)DD;
+      const uint32_t per = scan_f ? (uint32_t)nf : m * (uint32_t)DD;
       const uint32_t tp = (uint32_t)nl * per;
       merges += tp;
+      const float inv_per = 1.0f / (float)per;
+      const float inv_m = 1.0f / (float)m;
       for (uint32_t t = lane; t < tp; t += 32) {
-        const uint32_t a = t / per, r = t - a * per;
-        const uint32_t yb = r / DD + 1u, d2 = r - (yb - 1u) * DD;
+        const uint32_t a = udiv_small(t, per, inv_per), r = t - a * per;
         const uint32_t cell = list[a];
-        const uint32_t X = cell / DD, d1 = cell - X * DD;
+        const uint32_t X = cell & full, d1 = cell >> k;
+        uint32_t Y, d2;
+        if (scan_f) {
+          const uint32_t yc = flist[r];
+          Y = yc & full;
+          d2 = yc >> k;
+          if (Y & X) continue;
+        } else {
+          // r = d2 * m + (yb - 1): partner hop d2, partner = yb-th submask of ~X
+          d2 = udiv_small(r, m, inv_m);
+          Y = deposit(r - d2 * m + 1u, full ^ X);
+        }
         if (hop && (int)(d1 + d2) > D) continue;
-        const uint32_t Y = deposit(yb, full ^ X);
-        if (!in_bounds(c, Y * DD + d2 < (uint32_t)RW && (X | Y) * DD < (uint32_t)RW, 9)) continue;
-        const uint32_t cy = cost_of(buf[Y * DD + d2]);
+        if (!in_bounds(c, (d2 << k) + Y < (uint32_t)RW && (X | Y) < (uint32_t)W, 9)) continue;
+        const uint32_t cy = cost_of(buf[(d2 << k) + Y]);
         if (cy == COST_INF) continue;
         const uint32_t cand = cost_of(buf[cell]) + cy;
         const uint32_t S = X | Y;
         if (S != full && 3ull * cand > 2ull * ubm) continue;
         const uint32_t nd = d1 > d2 ? d1 : d2;
-        const uint32_t tgt = S * DD + nd;
+        const uint32_t tgt = (nd << k) + S;
         const uint64_t nv = pack_cell(cand, PEND | MERGE | Y | (d2 << 16) | (d1 << 21));
         if (nv < buf[tgt]) {
           const uint64_t old = atomicMin(&buf[tgt], (unsigned long long)nv);
-          if (nv < old) atomicOr(&pend[tgt >> 5], 1u << (tgt & 31));
+          if (nv < old) {
+            atomicOr(&pend[tgt >> 5], 1u << (tgt & 31));
+            atomicOr(&wcls[wib], 1u << __popc(S));
+          }
         }
       }
       __syncwarp();
     }
-    // one-label distances of v (non-hop, or hop with use_lb)
-    uint32_t dv[KMAX];
+    // one-label distances of v (non-hop, or hop with use_lb): lane g holds d_g(v).
+    // dv: distances as stored (path lengths, for the one-label upper bound); dl: the
+    // same clamped to cut + 1, lower bounds for the pruning tests
+    uint32_t dv[KMAX], dl[KMAX];
+    uint32_t lim = COST_INF, mine = COST_INF;
 #pragma unroll
-    for (int i = 0; i < KMAX; i++) dv[i] = COST_INF;
+    for (int i = 0; i < KMAX; i++) dv[i] = dl[i] = COST_INF;
     if (c->use_lb) {
-      const uint32_t mine = lane < k ? __ldcg(&c->dist[(uint64_t)v * DIST_STRIDE + lane]) : COST_INF;
+      mine = lane < k ? __ldcg(&c->dist[(uint64_t)v * DIST_STRIDE + lane]) : COST_INF;
+      const uint32_t cut = c->cut;
+      lim = cut == COST_INF ? COST_INF : cut + 1u;
 #pragma unroll
-      for (int i = 0; i < KMAX; i++) dv[i] = __shfl_sync(0xffffffffu, mine, i);
+      for (int i = 0; i < KMAX; i++) {
+        dv[i] = __shfl_sync(0xffffffffu, mine, i);
+        dl[i] = min(dv[i], lim);
+      }
     }
     const int64_t deg = G.beg[v + 1] - G.beg[v];
-    // settle changed states; emit growable ones
+    const int use_tour = c->use_tour;
+    // settle changed states (lane-parallel): write them back, update the full-set
+    // bounds, and apply the one-label and hop tests.  pend keeps the states that
+    // pass; those that still need the tour bound are listed for the warp below.
+    int ncand = 0;
     for (int i0 = 0; i0 < RW; i0 += 32) {
       const int i = i0 + lane;
+      bool keep = false, cand = false;
       if (i < RW && ((pend[i >> 5] >> (i & 31)) & 1u)) {
         const uint64_t x = buf[i];
         row[i] = x & ~(uint64_t)PEND;
         const uint32_t cst = cost_of(x);
-        const uint32_t p = (uint32_t)i / DD, d = (uint32_t)i - p * DD;
+        const uint32_t p = (uint32_t)i & full, d = (uint32_t)i >> k;
         if (p == full) {
           atomicMin(&c->best, ((unsigned long long)cst << 32) | ((unsigned long long)d << 27) | v);
           atomicMin(&c->ub_cell, cst);
@@ -585,7 +878,7 @@ __global__ void __launch_bounds__(256) k_rows(Ctx* ctxs, int nctx, DevGraph G, i
 #pragma unroll
             for (int b = 0; b < KMAX; b++)
               if (b < k && !((p >> b) & 1u)) {
-                lb = max(lb, dv[b]);
+                lb = max(lb, dl[b]);
                 one += dv[b];
               }
             if (!hop && one < (uint64_t)c->ub) atomicMin(&c->ub, (uint32_t)one);
@@ -593,47 +886,86 @@ __global__ void __launch_bounds__(256) k_rows(Ctx* ctxs, int nctx, DevGraph G, i
           const uint32_t bound = hop ? c->ub_cell : c->ub;
           bool grow = 2ull * cst <= (uint64_t)bound && (uint64_t)cst + lb <= (uint64_t)bound;
           if (hop) grow = grow && (int)d < D && cst < bound;
-          if (grow && c->use_tour) {
-            // tour bound of PrunedDP++ (code/PrunedDP++/include/CPUNONHOP.h:433-493):
-            // the rest of the tree, doubled, is a closed walk from v through every
-            // group of Xb = full \ p, so twice its cost is at least
-            //   min_{i,j} d_i(v) + P(i,j,Xb) + d_j(v)            and, for every i,
-            //   d_i(v) + min_j P(i,j,Xb) + min_j d_j(v),
-            // P = cheapest group sequence from i to j visiting each group of Xb once.
-            const uint32_t Xb = full ^ p;
-            const uint32_t* Wt = c->tour + (size_t)Xb * TOUR_STRIDE;
-            const uint32_t* W2 = c->tour + (size_t)c->W * TOUR_STRIDE + (size_t)Xb * KMAX;
-            uint64_t mind = COST_INF;
-#pragma unroll
-            for (int b = 0; b < KMAX; b++)
-              if (b < k && ((Xb >> b) & 1u) && dv[b] < mind) mind = dv[b];
-            uint64_t lb1 = ~0ull, lb2 = 0;
-#pragma unroll
-            for (int a = 0; a < KMAX; a++) {
-              if (a >= k || !((Xb >> a) & 1u)) continue;
-              const uint64_t t2 = (uint64_t)dv[a] + __ldg(&W2[a]) + mind;
-              if (t2 > lb2) lb2 = t2;
-#pragma unroll
-              for (int b = 0; b < KMAX; b++) {
-                if (b >= k || !((Xb >> b) & 1u)) continue;
-                const uint64_t t1 = (uint64_t)dv[a] + __ldg(&Wt[a * KMAX + b]) + dv[b];
-                if (t1 < lb1) lb1 = t1;
-              }
-            }
-            const uint64_t t = lb1 > lb2 ? lb1 : lb2;
-            grow = (uint64_t)cst + (t + 1) / 2 <= (uint64_t)bound;
+          if (grow && deg > 0) {
+            keep = true;
+            cand = use_tour != 0;
           }
-          if (grow && deg > 0)
-            push_state(c, v, p | (d << 16), cst, light_count(G, v, deg, grow_limit(c, cst)), split,
-                       c->bucket_end);
         }
       }
-    }
-    if (lane == 0) {
-      atomicAdd(&c->st_merge, (unsigned long long)merges);
-      atomicAdd(&c->st_rows, 1ull);
+      const uint32_t bk = __ballot_sync(0xffffffffu, keep);
+      const uint32_t bc = __ballot_sync(0xffffffffu, cand);
+      if (cand) list[ncand + __popc(bc & ((1u << lane) - 1u))] = (uint16_t)i;
+      ncand += __popc(bc);
+      if (lane == 0) pend[i0 >> 5] = bk;
     }
     __syncwarp();
+    if (ncand > 0) {
+      // tour bound of PrunedDP++ (code/PrunedDP++/include/CPUNONHOP.h:433-493): the
+      // rest of the tree, doubled, is a closed walk from v through every group of
+      // Xb = full \ p, so twice its cost is at least
+      //   min_{a,b} d_a(v) + P(a,b,Xb) + d_b(v)          and, for every a,
+      //   d_a(v) + min_b P(a,b,Xb) + min_b d_b(v),
+      // P = cheapest group sequence from a to b visiting each group of Xb once.
+      // One candidate at a time, the warp's lanes over the (a, b) pairs.
+      const int a0 = lane >> 3, bb = lane & 7;
+      const uint32_t dla = min(__shfl_sync(0xffffffffu, mine, a0), lim);
+      const uint32_t dla2 = min(__shfl_sync(0xffffffffu, mine, a0 + 4), lim);
+      const uint32_t dlb = min(__shfl_sync(0xffffffffu, mine, bb), lim);
+      const uint32_t bound = hop ? __ldcg(&c->ub_cell) : __ldcg(&c->ub);
+      for (int t = 0; t < ncand; t++) {
+        const uint32_t i = list[t];
+        const uint32_t p = i & full, cst = cost_of(buf[i]);
+        const uint32_t Xb = full ^ p;
+        const uint32_t* Wt = c->tour + (size_t)Xb * TOUR_STRIDE;
+        const uint32_t* W2 = c->tour + (size_t)c->W * TOUR_STRIDE + (size_t)Xb * KMAX;
+        const bool inA = a0 < k && ((Xb >> a0) & 1u);
+        const bool inA2 = a0 + 4 < k && ((Xb >> (a0 + 4)) & 1u);
+        const bool inB = bb < k && ((Xb >> bb) & 1u);
+        uint64_t t1 = ~0ull;
+        if (inA && inB) t1 = (uint64_t)dla + __ldg(&Wt[a0 * KMAX + bb]) + dlb;
+        if (inA2 && inB) t1 = min(t1, (uint64_t)dla2 + __ldg(&Wt[(a0 + 4) * KMAX + bb]) + dlb);
+        const uint32_t lb1 = __reduce_min_sync(0xffffffffu, (uint32_t)min(t1, (uint64_t)COST_INF));
+        const uint32_t mind = __reduce_min_sync(0xffffffffu, (lane < 8 && inB) ? dlb : COST_INF);
+        uint64_t t2 = 0;
+        if (lane < 8 && inB) t2 = (uint64_t)dlb + __ldg(&W2[bb]) + mind;
+        const uint32_t lb2 = __reduce_max_sync(0xffffffffu, (uint32_t)min(t2, (uint64_t)COST_INF));
+        const uint64_t tb = lb1 > lb2 ? lb1 : lb2;
+        if ((uint64_t)cst + (tb + 1) / 2 > (uint64_t)bound && lane == 0)
+          pend[i >> 5] &= ~(1u << (i & 31));
+        __syncwarp();
+      }
+    }
+    // emit the growing states, each relaxed from its lightest edge on (which lands
+    // at cst + 1 or later)
+    const uint32_t bend = c->bucket_end;
+    for (int i0 = 0; i0 < RW; i0 += 32) {
+      const int i = i0 + lane;
+      const bool want = i < RW && ((pend[i >> 5] >> (i & 31)) & 1u);
+      uint32_t gpd = 0, gcost = 0;
+      if (want) {
+        const uint32_t p = (uint32_t)i & full, d = (uint32_t)i >> k;
+        gpd = p | (d << 16);
+        gcost = cost_of(buf[i]);
+      }
+      warp_append(ctxs, qi, want, (uint64_t)gcost + 1u >= bend, v, gpd, gcost, 0u, gcost + 1u);
+    }
+    // statistics: one atomic per query change of the warp, not per row
+    if (qi != st_q) {
+      if (st_q >= 0 && lane == 0) {
+        atomicAdd(&ctxs[st_q].st_merge, (unsigned long long)st_merges);
+        atomicAdd(&ctxs[st_q].st_rows, (unsigned long long)st_rows);
+      }
+      st_q = qi;
+      st_merges = 0;
+      st_rows = 0;
+    }
+    st_merges += merges;
+    st_rows += 1;
+    __syncwarp();
+  }
+  if (st_q >= 0 && lane == 0) {
+    atomicAdd(&ctxs[st_q].st_merge, (unsigned long long)st_merges);
+    atomicAdd(&ctxs[st_q].st_rows, (unsigned long long)st_rows);
   }
 }
 
@@ -715,8 +1047,18 @@ __global__ void k_ctrl(Ctx* ctxs, int nctx, int mode) {
   if (qi >= nctx) return;
   Ctx* c = ctxs + qi;
   if (mode == CTRL_SSSP && c->phase == PH_PREP && !c->error) {
+    // The distances are final up to the cutoff ub: every stored distance <= ub is
+    // exact, and any other is only known to be > ub.  The group distances feed a
+    // lower bound, so they are clamped to ub + 1, a value never above the truth.
+    const uint32_t cut = c->ub;
+    const uint32_t lim = cut == COST_INF ? COST_INF : cut + 1u;
+    for (int i = threadIdx.x; i < KMAX * KMAX; i += blockDim.x) c->vv[i] = min(c->vv[i], lim);
+    __syncthreads();
     if (c->use_tour) build_tour(c);  // block-uniform branch
-    if (threadIdx.x == 0) ctrl_start_dp(c);
+    if (threadIdx.x == 0) {
+      c->cut = cut;
+      ctrl_start_dp(c);
+    }
     return;
   }
   if (threadIdx.x != 0) return;
@@ -738,6 +1080,7 @@ __global__ void k_ctrl(Ctx* ctxs, int nctx, int mode) {
     if (c->in_kind == 0) c->n_q[c->in_idx] = 0;
     else c->n_far[c->in_idx] = 0;
     const uint32_t s = c->no;
+    c->st_qmax = max(c->st_qmax, max(c->n_q[s], c->n_far[c->f]));
     if (c->n_q[s] > 0) {
       c->in_ptr = c->q[s];
       c->in_n = min(c->n_q[s], c->qcap);
@@ -754,13 +1097,18 @@ __global__ void k_ctrl(Ctx* ctxs, int nctx, int mode) {
       c->in_n = 0;
     }
   } else if (mode == CTRL_DP_ROWS) {
+    // the rows kernel appended the grow items of the states it settled to q[no]
+    // (after the continuations the last grow step appended there)
     if (c->phase != PH_DP) return;
     c->n_rows = 0;  // consumed by the rows kernel
-    if (c->n_q[0] > 0) {
-      c->in_ptr = c->q[0];
-      c->in_n = min(c->n_q[0], c->qcap);
+    const uint32_t s = c->no;
+    c->st_qmax = max(c->st_qmax, max(c->n_q[s], c->n_far[c->f]));
+    if (c->n_q[s] > 0) {
+      c->in_ptr = c->q[s];
+      c->in_n = min(c->n_q[s], c->qcap);
       c->in_kind = 0;
-      c->in_idx = 0;
+      c->in_idx = s;
+      c->no = s ^ 1u;
     } else if (c->n_far[c->f] > 0) {
       ctrl_take_far(c);
     } else {
@@ -775,9 +1123,34 @@ __global__ void k_ctrl(Ctx* ctxs, int nctx, int mode) {
       c->in_n = 0;
       return;
     }
-    if (c->in_kind == 0) c->n_q[0] = 0;
+    if (c->in_kind == 0) c->n_q[c->in_idx] = 0;
     else c->n_far[c->in_idx] = 0;
     c->in_n = 0;
+  }
+}
+
+// ---- device-side loop control of the level graph -----------------------------------
+// Last node of the level body of the CUDA graph's WHILE loop: go on while no
+// resident query has finished, some query is resident and iterations are left.
+// loop[0] = iterations left (host-set before the launch), loop[1] = a query finished.
+__global__ void k_loop_cond(const Ctx* ctxs, int nctx, uint32_t* loop,
+                            cudaGraphConditionalHandle h) {
+  const int i = threadIdx.x;  // blockDim.x >= MAXB
+  bool fin = false, act = false;
+  if (i < nctx) {
+    const Ctx* c = ctxs + i;
+    if (!c->idle) {
+      act = true;
+      fin = c->phase >= PH_DONE;
+    }
+  }
+  const int any_fin = __syncthreads_or(fin);
+  const int any_act = __syncthreads_or(act);
+  if (i == 0) {
+    const uint32_t left = loop[0] > 0 ? loop[0] - 1u : 0u;
+    loop[0] = left;
+    loop[1] = any_fin ? 1u : 0u;
+    cudaGraphSetConditional(h, (!any_fin && any_act && left > 0) ? 1u : 0u);
   }
 }
 
@@ -805,8 +1178,9 @@ __global__ void k_extract(Ctx* ctxs, int nctx, DevGraph G) {
   const uint32_t d0 = (uint32_t)((c->best >> 27) & 31u);
   const uint64_t RW = (uint64_t)c->RW;
   const uint32_t DD = (uint32_t)c->DD;
+  const int k = c->k;
   uint32_t sp = 0, nout = 0, steps = 0;
-  c->stack[sp++] = (uint64_t)v0 * RW + (uint64_t)c->full * DD + d0;
+  c->stack[sp++] = (uint64_t)v0 * RW + ((uint64_t)d0 << k) + (uint64_t)c->full;
   while (sp > 0) {
     if (++steps > 4u * c->stackcap) {
       c->error |= ERR_EXTRACT;
@@ -816,7 +1190,7 @@ __global__ void k_extract(Ctx* ctxs, int nctx, DevGraph G) {
     if (!in_bounds(c, idx < (uint64_t)G.V * RW, 10)) break;
     const uint32_t v = (uint32_t)(idx / RW);
     const uint32_t r = (uint32_t)(idx - (uint64_t)v * RW);
-    const uint32_t p = r / DD, d = r - p * DD;
+    const uint32_t p = r & (uint32_t)c->full, d = r >> k;
     const uint64_t cell = c->table[idx];
     const uint32_t par = (uint32_t)cell & ~PEND;
     if (cost_of(cell) == COST_INF) {  // a parent pointer never leads to an unreached state
@@ -840,7 +1214,7 @@ __global__ void k_extract(Ctx* ctxs, int nctx, DevGraph G) {
         c->error |= ERR_EXTRACT;
         break;
       }
-      c->stack[sp++] = (uint64_t)u * RW + (uint64_t)p * DD + (d - (uint32_t)c->hop);
+      c->stack[sp++] = (uint64_t)u * RW + ((uint64_t)(d - (uint32_t)c->hop) << k) + p;
     } else {
       const uint32_t Y = par & 0xFFFFu, d2 = (par >> 16) & 31u, d1 = (par >> 21) & 31u;
       const uint32_t X = p ^ Y;
@@ -852,8 +1226,8 @@ __global__ void k_extract(Ctx* ctxs, int nctx, DevGraph G) {
         c->error |= ERR_EXTRACT;
         break;
       }
-      c->stack[sp++] = (uint64_t)v * RW + (uint64_t)X * DD + d1;
-      c->stack[sp++] = (uint64_t)v * RW + (uint64_t)Y * DD + d2;
+      c->stack[sp++] = (uint64_t)v * RW + ((uint64_t)d1 << k) + X;
+      c->stack[sp++] = (uint64_t)v * RW + ((uint64_t)d2 << k) + Y;
     }
   }
   if (nout > c->outcap) c->error |= ERR_EXTRACT;

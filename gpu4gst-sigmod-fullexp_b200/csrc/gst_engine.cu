@@ -1,19 +1,32 @@
 // Host side of the GST engine and its C ABI (include/gst.h).
 //
-// A gst_graph owns the device CSR and a pool of query slots (state slab,
-// one-label distances, worklists).  gst_solve runs one query in slot 0;
-// gst_solve_batch runs up to cfg.max_batch queries at once in as many slots,
-// refilling a slot as soon as its query finishes.  The level loop is a fixed
-// launch sequence (sssp, ctrl, rows, ctrl, grow, ctrl) that the host issues a few
-// levels ahead of the device; every kernel reads its work counts from the
-// device-side contexts, so extra launches after a query finishes are no-ops.
+// A gst_graph owns the device CSR.  Queries run in a Runner: a set of resident
+// query slots (state slab, one-label distances, worklists, control context) that
+// share every launch of the level loop.  gst_solve_batch drives a runner from a
+// list of queries; a gst_server drives its own runner from a submission queue on a
+// host thread, admitting new queries at level boundaries (continuous batching).
+// Slot memory comes from the engine's stream-ordered memory pool and is admitted
+// against a memory budget by the size of each query's state table.
+//
+// The level loop is a fixed launch sequence (sssp, ctrl, rows, ctrl, grow, ctrl)
+// that every resident query steps through together; each kernel reads its work
+// counts from the device-side contexts, so launches after a query finishes are
+// no-ops for it.  The host either issues a few levels ahead and then reads the
+// contexts back, or (cfg.use_graphs) launches one CUDA graph whose conditional
+// WHILE node repeats the level body on the device until a query finishes.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <condition_variable>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -28,9 +41,15 @@ namespace {
 
 thread_local std::string tl_err;
 
-struct Slot {
-  size_t rw_cap = 0;     // cells per row the slab was sized for
-  int64_t V = 0;
+using Clock = std::chrono::steady_clock;
+
+// Device memory of one query slot: one pool allocation carved into the buffers.
+struct SlotMem {
+  void* base = nullptr;
+  size_t bytes = 0;
+  size_t rw = 0;          // cells per row the slab holds
+  uint32_t cap = 0;       // near-list capacity (items)
+  uint32_t farcap = 0;    // far-list capacity (0 when the frontier has one bucket)
   uint64_t* table = nullptr;
   uint32_t* dist = nullptr;
   uint32_t* rowbits = nullptr;
@@ -40,31 +59,79 @@ struct Slot {
   uint32_t* rows = nullptr;
   int32_t* out = nullptr;
   uint64_t* stack = nullptr;
-  uint32_t qcap = 0, farcap = 0, rowcap = 0, outcap = 0, stackcap = 0;
-  size_t bytes = 0;
+  uint32_t rowcap = 0, outcap = 0, stackcap = 0;
 };
+
+constexpr size_t kTourWords = ((size_t)1 << KMAX) * (TOUR_STRIDE + KMAX);
+constexpr uint32_t kOutCap = 1u << 16;
+constexpr uint32_t kStackCap = 1u << 18;
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Lay out (or, with base == nullptr, only size) a slot of V rows of rw cells.
+size_t carve_slot(SlotMem& m, unsigned char* base, int64_t V, size_t rw, uint32_t cap,
+                  uint32_t farcap) {
+  size_t off = 0;
+  auto take = [&](size_t n) {
+    unsigned char* p = base ? base + off : nullptr;
+    off = align256(off + n);
+    return p;
+  };
+  m.table = (uint64_t*)take((size_t)V * rw * 8);
+  m.dist = (uint32_t*)take((size_t)V * DIST_STRIDE * 4);
+  m.rowbits = (uint32_t*)take(((size_t)V + 31) / 32 * 4);
+  m.tour = (uint32_t*)take(kTourWords * 4);
+  m.q[0] = (uint4*)take((size_t)cap * 16);
+  m.q[1] = (uint4*)take((size_t)cap * 16);
+  m.far[0] = (uint4*)take((size_t)farcap * 16);
+  m.far[1] = (uint4*)take((size_t)farcap * 16);
+  m.rows = (uint32_t*)take((size_t)V * 4);
+  m.out = (int32_t*)take((size_t)kOutCap * 12);
+  m.stack = (uint64_t*)take((size_t)kStackCap * 8);
+  m.rw = rw;
+  m.cap = cap;
+  m.farcap = farcap;
+  m.rowcap = (uint32_t)V;
+  m.outcap = kOutCap;
+  m.stackcap = kStackCap;
+  return off;
+}
+
+size_t row_width(int k, int D) { return ((size_t)1 << k) * (size_t)(D >= 0 ? D + 1 : 1); }
+
+// Worklist capacity.  A level appends at most one item per edge chunk of every
+// state it settles, which in the worst case is every cell of the slab; queries
+// use a small fraction of that, so a slot starts at `base` items and a query that
+// overflows is re-run with four times the room (up to the worst case).
+uint32_t list_cap(int64_t V, int64_t E, size_t rw, int split, int boost) {
+  const uint64_t worst = std::min<uint64_t>((uint64_t)V * rw + (uint64_t)E / split * rw + 4096,
+                                            (1ull << 31));
+  uint64_t c = std::max<uint64_t>(1ull << 16, 4ull * (uint64_t)V + 2ull * (uint64_t)E / split);
+  for (int i = 0; i < boost; i++) c *= 4;
+  return (uint32_t)std::min(c, worst);
+}
+bool cap_is_worst(int64_t V, int64_t E, size_t rw, int split, uint32_t cap) {
+  return cap >= std::min<uint64_t>((uint64_t)V * rw + (uint64_t)E / split * rw + 4096, 1ull << 31);
+}
 
 }  // namespace
-
-// Counters of one gst_solve_batch call.
-struct CallStats {
-  int64_t launches = 0, h2d = 0, d2h = 0;
-  std::vector<std::pair<int, int>> prof;  // (kernel kind, event-pair index)
-  size_t next_ev = 0;
-};
 
 struct gst_engine {
   int device = 0;
   gst_config cfg{};
   cudaStream_t stream = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  std::vector<cudaEvent_t> prof_events;  // reused pairs for cfg.profile_kernels
-  CallStats cs;
+  cudaMemPool_t pool = nullptr;
+  std::vector<cudaEvent_t> prof_events;  // reused start/stop pairs for cfg.profile_kernels
   int sms = 148;
   int grow_blocks = 0, sssp_blocks = 0;
+  std::vector<std::pair<uint64_t, int>> rows_occ;  // (threads<<32 | smem) -> grid
   std::string err;
-  std::mutex mu;
+  std::mutex mu;                                   // serialises all GPU work of the engine
 };
+
+namespace {
+struct Runner;
+}
 
 struct gst_graph {
   gst_engine* eng = nullptr;
@@ -73,10 +140,7 @@ struct gst_graph {
   int2* d_edges = nullptr;   // per vertex sorted by neighbour (tree extraction)
   int2* d_wedges = nullptr;  // per vertex sorted by (weight, neighbour) (grow, SSSP)
   uint32_t* d_widx = nullptr;
-  std::vector<int64_t> h_beg;
-  std::vector<Slot> slots;
-  Ctx* d_ctx = nullptr;       // MAXB contexts
-  Ctx* h_ctx = nullptr;       // pinned mirror
+  std::unique_ptr<Runner> batch;  // runner of gst_solve / gst_solve_batch (slots kept)
 };
 
 struct gst_groups {
@@ -103,67 +167,7 @@ gst_status fail(gst_engine* e, gst_status s, const std::string& msg) {
                   std::string(#call) + ": " + cudaGetErrorString(_e));                \
   } while (0)
 
-void free_slot(Slot& s) {
-  cudaFree(s.table);
-  cudaFree(s.dist);
-  cudaFree(s.rowbits);
-  cudaFree(s.tour);
-  cudaFree(s.q[0]);
-  cudaFree(s.q[1]);
-  cudaFree(s.far[0]);
-  cudaFree(s.far[1]);
-  cudaFree(s.rows);
-  cudaFree(s.out);
-  cudaFree(s.stack);
-  s = Slot();
-}
-
-// worklist capacity for a slab of V rows of rw cells
-uint32_t list_cap(int64_t V, size_t rw) {
-  const uint64_t want = (uint64_t)V * rw + 4ull * (uint64_t)V + 4096;
-  return (uint32_t)std::min<uint64_t>(want, 1ull << 26);
-}
-
-constexpr size_t kTourWords = ((size_t)1 << KMAX) * (TOUR_STRIDE + KMAX);
-
-size_t slot_bytes(int64_t V, size_t rw) {
-  const uint64_t cap = list_cap(V, rw);
-  return (size_t)V * rw * 8 + (size_t)V * DIST_STRIDE * 4 + ((size_t)V + 31) / 32 * 4 +
-         kTourWords * 4 +
-         4 * (size_t)cap * 16 + (size_t)V * 4 + (size_t)(1 << 16) * 12 + (size_t)(1 << 18) * 8;
-}
-
-gst_status ensure_slot(gst_engine* eng, gst_graph* g, size_t idx, size_t rw) {
-  if (g->slots.size() <= idx) g->slots.resize(idx + 1);
-  Slot& s = g->slots[idx];
-  if (s.table && s.rw_cap >= rw && s.V == g->V) return GST_OK;
-  free_slot(s);
-  const int64_t V = g->V;
-  s.V = V;
-  s.rw_cap = rw;
-  s.qcap = s.farcap = list_cap(V, rw);
-  s.rowcap = (uint32_t)V;
-  s.outcap = 1 << 16;
-  s.stackcap = 1 << 18;
-  CK(cudaMalloc(&s.table, (size_t)V * rw * 8));
-  CK(cudaMalloc(&s.dist, (size_t)V * DIST_STRIDE * 4));
-  CK(cudaMalloc(&s.rowbits, ((size_t)V + 31) / 32 * 4));
-  CK(cudaMalloc(&s.tour, kTourWords * 4));
-  for (int i = 0; i < 2; i++) {
-    CK(cudaMalloc(&s.q[i], (size_t)s.qcap * 16));
-    CK(cudaMalloc(&s.far[i], (size_t)s.farcap * 16));
-  }
-  CK(cudaMalloc(&s.rows, (size_t)V * 4));
-  CK(cudaMalloc(&s.out, (size_t)s.outcap * 12));
-  CK(cudaMalloc(&s.stack, (size_t)s.stackcap * 8));
-  CK(cudaMemsetAsync(s.rowbits, 0, ((size_t)V + 31) / 32 * 4, eng->stream));
-  s.bytes = slot_bytes(V, rw);
-  return GST_OK;
-}
-
-size_t row_width(int k, int D) { return ((size_t)1 << k) * (size_t)(D >= 0 ? D + 1 : 1); }
-
-gst_status validate_query(gst_engine* eng, gst_groups* grp, const gst_query* q) {
+gst_status validate_query(gst_engine* eng, const gst_groups* grp, const gst_query* q) {
   if (!q || q->k < 1 || q->k > KMAX || !q->group_ids)
     return fail(eng, GST_BAD_INPUT, "query: k must be in [1,8] with group ids");
   if (q->hop_bound > 30) return fail(eng, GST_BAD_INPUT, "query: hop bound must be <= 30");
@@ -178,117 +182,6 @@ gst_status validate_query(gst_engine* eng, gst_groups* grp, const gst_query* q) 
   return GST_OK;
 }
 
-// Host copy of a fresh context for query q in slot s.
-void prep_ctx(gst_engine* eng, gst_graph* g, Slot& s, const gst_query* q, Ctx& c) {
-  memset(&c, 0, sizeof(c));
-  const int hop = q->hop_bound >= 0;
-  c.table = s.table;
-  c.dist = s.dist;
-  c.rowbits = s.rowbits;
-  c.tour = s.tour;
-  c.q[0] = s.q[0];
-  c.q[1] = s.q[1];
-  c.far[0] = s.far[0];
-  c.far[1] = s.far[1];
-  c.rows = s.rows;
-  c.out = s.out;
-  c.stack = s.stack;
-  c.qcap = s.qcap;
-  c.farcap = s.farcap;
-  c.rowcap = s.rowcap;
-  c.outcap = s.outcap;
-  c.stackcap = s.stackcap;
-  c.k = q->k;
-  c.W = 1 << q->k;
-  c.full = c.W - 1;
-  c.D = hop ? q->hop_bound : 0;
-  c.DD = hop ? q->hop_bound + 1 : 1;
-  c.RW = c.W * c.DD;
-  c.hop = hop;
-  c.use_lb = hop ? 0 : 1;
-  c.use_tour = c.use_lb;
-  for (int i = 0; i < q->k; i++) c.gid[i] = q->group_ids[i];
-  memset(c.vv, 0xFF, sizeof(c.vv));
-  c.delta = (uint32_t)std::max(0, eng->cfg.bucket_delta);
-  c.max_levels = (uint32_t)eng->cfg.max_levels;
-  c.in_ptr = nullptr;
-  c.in_n = 0;
-  c.in_kind = 0;
-  c.in_idx = 1;
-  c.no = 0;
-  c.f = 0;
-  c.far_min = 0xFFFFFFFFu;
-  c.bucket_end = c.delta ? c.delta : 0xFFFFFFFFu;
-  c.ub = 0xFFFFFFFFu;
-  c.ub_cell = 0xFFFFFFFFu;
-  c.best = ~0ull;
-  c.phase = c.use_lb ? PH_SSSP : PH_DP;
-}
-
-// Clear the slot's slab and distances for a query with row width rw.
-gst_status reset_slot(gst_engine* eng, gst_graph* g, Slot& s, size_t rw, bool need_dist) {
-  CK(cudaMemsetAsync(s.table, 0xFF, (size_t)g->V * rw * 8, eng->stream));
-  CK(cudaMemsetAsync(s.rowbits, 0, ((size_t)g->V + 31) / 32 * 4, eng->stream));
-  if (need_dist) CK(cudaMemsetAsync(s.dist, 0xFF, (size_t)g->V * DIST_STRIDE * 4, eng->stream));
-  return GST_OK;
-}
-
-struct LoopShape {
-  bool sssp = true;
-  int rw_max = 1;
-};
-
-enum ProfKind { PROF_GROW = 0, PROF_ROWS = 1, PROF_SSSP = 2 };
-
-// Record the start event of a profiled launch; returns the pair index or -1.
-int prof_begin(gst_engine* eng, int kind) {
-  if (!((eng->cfg.profile_kernels >> kind) & 1)) return -1;
-  const size_t i = eng->cs.next_ev++;
-  while (eng->prof_events.size() < 2 * (i + 1)) {
-    cudaEvent_t e;
-    if (cudaEventCreate(&e) != cudaSuccess) return -1;
-    eng->prof_events.push_back(e);
-  }
-  cudaEventRecord(eng->prof_events[2 * i], eng->stream);
-  eng->cs.prof.push_back({kind, (int)i});
-  return (int)i;
-}
-void prof_end(gst_engine* eng, int i) {
-  if (i >= 0) cudaEventRecord(eng->prof_events[2 * i + 1], eng->stream);
-}
-
-DevGraph dev_graph(const gst_graph* g) {
-  return DevGraph{g->V, g->E, g->d_beg, g->d_edges, g->d_wedges, g->d_widx};
-}
-
-gst_status launch_level(gst_engine* eng, gst_graph* g, int nctx, const LoopShape& sh) {
-  cudaStream_t st = eng->stream;
-  const DevGraph G = dev_graph(g);
-  const int split = eng->cfg.split_degree;
-  const int tpb = eng->cfg.threads_per_block;
-  if (sh.sssp) {
-    const int pe = prof_begin(eng, PROF_SSSP);
-    k_sssp<<<eng->sssp_blocks, 256, 0, st>>>(g->d_ctx, nctx, G, split);
-    prof_end(eng, pe);
-    k_ctrl<<<nctx, 128, 0, st>>>(g->d_ctx, nctx, CTRL_SSSP);
-    eng->cs.launches += 2;
-  }
-  const size_t per_warp = rows_smem_per_warp(sh.rw_max);
-  const int warps = std::max(1, tpb / 32);
-  int pe = prof_begin(eng, PROF_ROWS);
-  k_rows<<<eng->grow_blocks, warps * 32, per_warp * warps, st>>>(g->d_ctx, nctx, G, split,
-                                                                  sh.rw_max);
-  prof_end(eng, pe);
-  k_ctrl<<<nctx, 128, 0, st>>>(g->d_ctx, nctx, CTRL_DP_ROWS);
-  pe = prof_begin(eng, PROF_GROW);
-  k_grow<<<eng->grow_blocks, 256, 0, st>>>(g->d_ctx, nctx, G, split);
-  prof_end(eng, pe);
-  k_ctrl<<<nctx, 128, 0, st>>>(g->d_ctx, nctx, CTRL_DP_GROW);
-  eng->cs.launches += 4;
-  CK(cudaGetLastError());
-  return GST_OK;
-}
-
 gst_status status_of(const Ctx& c) {
   if (c.error & ERR_TIMEOUT) return GST_TIMEOUT;
   if (c.error & (ERR_QCAP | ERR_FARCAP | ERR_ROWCAP)) return GST_CAPACITY;
@@ -298,43 +191,625 @@ gst_status status_of(const Ctx& c) {
   return GST_OK;
 }
 
-void fill_result(gst_graph* g, const Ctx& c, const gst_query* q, const std::vector<int32_t>& raw,
-                 gst_result* r) {
-  memset(r, 0, sizeof(*r));
-  r->user_tag = q->user_tag;
-  r->status = status_of(c);
-  r->stats.levels = c.levels;
-  r->stats.states_expanded = (int64_t)c.st_items;
-  r->stats.edge_relaxations = (int64_t)c.st_relax;
-  r->stats.merge_pairs = (int64_t)c.st_merge;
-  r->stats.rows_merged = (int64_t)c.st_rows;
-  r->stats.sssp_relaxations = (int64_t)c.st_sssp;
-  if (r->status != GST_OK) return;
-  r->cost = (int32_t)(c.best >> 32);
-  r->root = (int32_t)(c.best & 0x7FFFFFFull);
-  r->root_hop = (int32_t)((c.best >> 27) & 31u);
-  // distinct edges, (min, max) orientation
-  std::vector<std::pair<std::pair<int32_t, int32_t>, int32_t>> es;
-  const size_t n = std::min<size_t>(c.n_out, raw.size() / 3);
-  es.reserve(n);
-  for (size_t i = 0; i < n; i++) {
-    int32_t a = raw[3 * i], b = raw[3 * i + 1];
-    if (a > b) std::swap(a, b);
-    es.push_back({{a, b}, raw[3 * i + 2]});
+DevGraph dev_graph(const gst_graph* g) {
+  return DevGraph{g->V, g->E, g->d_beg, g->d_edges, g->d_wedges, g->d_widx};
+}
+
+// Grid of the rows kernel: every SM filled with as many CTAs as its registers and
+// shared memory allow (the dynamic shared memory grows with the row width), capped
+// at cfg.blocks_per_sm.
+int rows_blocks(gst_engine* eng, int threads, size_t smem) {
+  const uint64_t key = ((uint64_t)threads << 32) | (uint64_t)smem;
+  for (auto& kv : eng->rows_occ)
+    if (kv.first == key) return kv.second;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rows, threads, smem) != cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  const int blocks = eng->sms * std::min(per_sm, std::max(1, eng->cfg.blocks_per_sm));
+  eng->rows_occ.push_back({key, blocks});
+  return blocks;
+}
+
+enum ProfKind { PROF_GROW = 0, PROF_ROWS = 1, PROF_SSSP = 2 };
+
+// A query waiting for, or holding, a slot.
+struct Job {
+  gst_query q{};
+  int32_t gids[KMAX] = {0};
+  gst_result* out = nullptr;     // destination of the result
+  uint64_t ticket = 0;
+  Clock::time_point t_submit;
+  int boost = 0;                 // worklist capacity boost (capacity retries)
+  size_t rw = 0;
+  std::atomic<bool> done{false};
+};
+
+// Per-call accounting (launches, bytes moved, profiled kernel time).
+struct CallStats {
+  int64_t launches = 0, h2d = 0, d2h = 0;
+  int64_t graph_launches = 0, graph_levels = 0;
+  std::vector<std::pair<int, int>> prof;  // (kernel kind, event-pair index)
+  size_t next_ev = 0;
+};
+
+// Resident query slots and the level loop over them.
+struct Runner {
+  gst_engine* eng;
+  gst_graph* g;
+  gst_groups* grp = nullptr;
+  int max_slots;
+  size_t budget = 0;            // bytes of slot memory the runner may hold
+  size_t held = 0;              // bytes of slot memory held now
+  Ctx* d_ctx = nullptr;         // MAXB contexts
+  Ctx* h_ctx = nullptr;         // pinned mirror
+  uint32_t* d_loop = nullptr;   // graph loop: {iterations left, any query finished}
+  uint32_t* loop_init = nullptr;  // pinned: values for d_loop before a launch
+  uint32_t* loop_left = nullptr;  // pinned: iterations left after it
+  std::vector<SlotMem> mem;
+  std::vector<Job*> owner;      // slot -> job (nullptr = free)
+  std::vector<uint8_t> idle_written;
+  int nctx = 0;                 // slots the kernels scan (high-water mark)
+  int active = 0;
+  CallStats cs;
+  // CUDA graphs of the level loop, by (nctx, rw_max)
+  struct LoopGraph {
+    int nctx;
+    int rw_max;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+  };
+  std::vector<LoopGraph> graphs;
+
+  Runner(gst_engine* e, gst_graph* gr, int slots) : eng(e), g(gr), max_slots(slots) {}
+  ~Runner() { release(); }
+
+  void release() {
+    cudaSetDevice(eng->device);
+    cudaStreamSynchronize(eng->stream);
+    for (auto& lg : graphs) {
+      if (lg.exec) cudaGraphExecDestroy(lg.exec);
+      if (lg.graph) cudaGraphDestroy(lg.graph);
+    }
+    graphs.clear();
+    for (auto& m : mem)
+      if (m.base) cudaFreeAsync(m.base, eng->stream);
+    cudaStreamSynchronize(eng->stream);
+    mem.clear();
+    held = 0;
+    if (d_ctx) cudaFree(d_ctx);
+    if (h_ctx) cudaFreeHost(h_ctx);
+    if (d_loop) cudaFree(d_loop);
+    if (loop_init) cudaFreeHost(loop_init);
+    loop_init = loop_left = nullptr;
+    d_ctx = nullptr;
+    h_ctx = nullptr;
+    d_loop = nullptr;
   }
-  std::sort(es.begin(), es.end());
-  es.erase(std::unique(es.begin(), es.end(),
-                       [](const auto& x, const auto& y) { return x.first == y.first; }),
-           es.end());
-  r->n_edges = (int64_t)es.size();
-  if (!es.empty()) {
-    r->edge_u = (int32_t*)malloc(sizeof(int32_t) * es.size());
-    r->edge_v = (int32_t*)malloc(sizeof(int32_t) * es.size());
-    r->edge_w = (int32_t*)malloc(sizeof(int32_t) * es.size());
-    for (size_t i = 0; i < es.size(); i++) {
-      r->edge_u[i] = es[i].first.first;
-      r->edge_v[i] = es[i].first.second;
-      r->edge_w[i] = es[i].second;
+
+  gst_status init() {
+    CK(cudaMalloc(&d_ctx, sizeof(Ctx) * MAXB));
+    CK(cudaMallocHost(&h_ctx, sizeof(Ctx) * MAXB));
+    CK(cudaMalloc(&d_loop, sizeof(uint32_t) * 4));
+    CK(cudaMallocHost(&loop_init, sizeof(uint32_t) * 4));
+    loop_left = loop_init + 2;
+    mem.assign(max_slots, SlotMem());
+    owner.assign(max_slots, nullptr);
+    idle_written.assign(max_slots, 0);
+    size_t free_b = 0, total_b = 0;
+    CK(cudaMemGetInfo(&free_b, &total_b));
+    budget = eng->cfg.mem_budget_bytes > 0 ? (size_t)eng->cfg.mem_budget_bytes
+                                           : (size_t)(free_b * 0.85);
+    return GST_OK;
+  }
+
+  size_t job_bytes(const Job& j) const {
+    SlotMem tmp;
+    const int split = eng->cfg.split_degree;
+    const uint32_t cap = list_cap(g->V, g->E, j.rw, split, j.boost);
+    return carve_slot(tmp, nullptr, g->V, j.rw, cap, eng->cfg.bucket_delta > 0 ? cap : 0);
+  }
+
+  int rw_max() const {
+    size_t r = 1;
+    for (int s = 0; s < nctx; s++)
+      if (owner[s]) r = std::max(r, mem[s].rw);
+    return (int)r;
+  }
+
+  // Free the memory of slots without a query, largest first, until `need` more
+  // bytes fit the budget.
+  void evict_idle(size_t need) {
+    while (held + need > budget) {
+      int best = -1;
+      for (int s = 0; s < (int)mem.size(); s++)
+        if (!owner[s] && mem[s].base && (best < 0 || mem[s].bytes > mem[best].bytes)) best = s;
+      if (best < 0) return;
+      cudaFreeAsync(mem[best].base, eng->stream);
+      held -= mem[best].bytes;
+      mem[best] = SlotMem();
+    }
+  }
+
+  // Put job j into a free slot.  GST_OK: admitted.  GST_NOT_READY: no slot or
+  // memory free now (retry after a query finishes).  GST_OOM_ADMISSION: the
+  // query's state table can never fit the budget.
+  gst_status admit(Job* j) {
+    const int split = eng->cfg.split_degree;
+    const uint32_t cap = list_cap(g->V, g->E, j->rw, split, j->boost);
+    const uint32_t farcap = eng->cfg.bucket_delta > 0 ? cap : 0;
+    const size_t need = job_bytes(*j);
+    if (need > budget) return GST_OOM_ADMISSION;
+    // the lowest free slot whose memory already fits (low slots keep the contexts
+    // the kernels scan few), else the lowest free slot
+    int s = -1;
+    for (int i = 0; i < max_slots && s < 0; i++)
+      if (!owner[i] && mem[i].base && mem[i].rw >= j->rw && mem[i].cap >= cap &&
+          mem[i].farcap >= farcap)
+        s = i;
+    if (s < 0) {
+      for (int i = 0; i < max_slots && s < 0; i++)
+        if (!owner[i]) s = i;
+      if (s < 0) return GST_NOT_READY;
+      if (mem[s].base) {
+        cudaFreeAsync(mem[s].base, eng->stream);
+        held -= mem[s].bytes;
+        mem[s] = SlotMem();
+      }
+      evict_idle(need);
+      if (held + need > budget) return GST_NOT_READY;
+      void* p = nullptr;
+      CK(cudaMallocFromPoolAsync(&p, need, eng->pool, eng->stream));
+      SlotMem m;
+      carve_slot(m, (unsigned char*)p, g->V, j->rw, cap, farcap);
+      m.base = p;
+      m.bytes = need;
+      mem[s] = m;
+      held += need;
+    }
+    SlotMem& m = mem[s];
+    // fresh context
+    Ctx& c = h_ctx[s];
+    memset(&c, 0, sizeof(c));
+    const gst_query* q = &j->q;
+    const int hop = q->hop_bound >= 0;
+    c.table = m.table;
+    c.dist = m.dist;
+    c.rowbits = m.rowbits;
+    c.tour = m.tour;
+    c.q[0] = m.q[0];
+    c.q[1] = m.q[1];
+    c.far[0] = m.far[0];
+    c.far[1] = m.far[1];
+    c.rows = m.rows;
+    c.out = m.out;
+    c.stack = m.stack;
+    c.qcap = cap;
+    c.farcap = farcap;
+    c.rowcap = m.rowcap;
+    c.outcap = m.outcap;
+    c.stackcap = m.stackcap;
+    c.k = q->k;
+    c.W = 1 << q->k;
+    c.full = c.W - 1;
+    c.D = hop ? q->hop_bound : 0;
+    c.DD = hop ? q->hop_bound + 1 : 1;
+    c.RW = c.W * c.DD;
+    c.hop = hop;
+    c.use_lb = hop ? 0 : 1;
+    c.use_tour = c.use_lb;
+    for (int i = 0; i < q->k; i++) c.gid[i] = q->group_ids[i];
+    memset(c.vv, 0xFF, sizeof(c.vv));
+    c.delta = (uint32_t)std::max(0, eng->cfg.bucket_delta);
+    c.max_levels = (uint32_t)eng->cfg.max_levels;
+    c.in_idx = 1;
+    c.far_min = 0xFFFFFFFFu;
+    c.bucket_end = c.delta ? c.delta : 0xFFFFFFFFu;
+    c.ub = 0xFFFFFFFFu;
+    c.cut = 0xFFFFFFFFu;
+    c.ub_cell = 0xFFFFFFFFu;
+    c.best = ~0ull;
+    c.phase = c.use_lb ? PH_SSSP : PH_DP;
+    cudaStream_t st = eng->stream;
+    CK(cudaMemsetAsync(m.table, 0xFF, (size_t)g->V * (size_t)c.RW * 8, st));
+    CK(cudaMemsetAsync(m.rowbits, 0, ((size_t)g->V + 31) / 32 * 4, st));
+    if (c.use_lb) CK(cudaMemsetAsync(m.dist, 0xFF, (size_t)g->V * DIST_STRIDE * 4, st));
+    CK(cudaMemcpyAsync(d_ctx + s, &c, sizeof(Ctx), cudaMemcpyHostToDevice, st));
+    cs.h2d += sizeof(Ctx) + sizeof(int32_t) * q->k;
+    const DevGraph G = dev_graph(g);
+    k_init<<<dim3(64, 1), 256, 0, st>>>(d_ctx + s, 1, G, grp->d_ptr, grp->d_mem,
+                                       eng->cfg.split_degree);
+    k_ctrl<<<1, 32, 0, st>>>(d_ctx + s, 1, CTRL_SSSP);
+    cs.launches += 2;
+    owner[s] = j;
+    idle_written[s] = 0;
+    nctx = std::max(nctx, s + 1);
+    active++;
+    return GST_OK;
+  }
+
+  // Contexts of free slots below nctx must look idle to the kernels.
+  gst_status write_idle() {
+    for (int s = 0; s < nctx; s++)
+      if (!owner[s] && !idle_written[s]) {
+        Ctx& c = h_ctx[s];
+        memset(&c, 0, sizeof(c));
+        c.phase = PH_DONE;
+        c.idle = 1;
+        c.best = ~0ull;
+        CK(cudaMemcpyAsync(d_ctx + s, &c, sizeof(Ctx), cudaMemcpyHostToDevice, eng->stream));
+        cs.h2d += sizeof(Ctx);
+        idle_written[s] = 1;
+      }
+    return GST_OK;
+  }
+
+  int prof_begin(int kind) {
+    if (!((eng->cfg.profile_kernels >> kind) & 1)) return -1;
+    const size_t i = cs.next_ev++;
+    while (eng->prof_events.size() < 2 * (i + 1)) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) return -1;
+      eng->prof_events.push_back(e);
+    }
+    cudaEventRecord(eng->prof_events[2 * i], eng->stream);
+    cs.prof.push_back({kind, (int)i});
+    return (int)i;
+  }
+  void prof_end(int i) {
+    if (i >= 0) cudaEventRecord(eng->prof_events[2 * i + 1], eng->stream);
+  }
+
+  // One level of every resident query: sssp, ctrl, rows, ctrl, grow, ctrl.
+  void launch_level(cudaStream_t st, int rwm, bool sssp, bool prof) {
+    const DevGraph G = dev_graph(g);
+    const int split = eng->cfg.split_degree;
+    const int tpb = eng->cfg.threads_per_block;
+    if (sssp) {
+      const int pe = prof ? prof_begin(PROF_SSSP) : -1;
+      k_sssp<<<eng->sssp_blocks, 256, 0, st>>>(d_ctx, nctx, G, split);
+      prof_end(pe);
+      k_ctrl<<<nctx, 128, 0, st>>>(d_ctx, nctx, CTRL_SSSP);
+    }
+    const size_t per_warp = rows_smem_per_warp(rwm);
+    const int warps = std::max(1, tpb / 32);
+    int pe = prof ? prof_begin(PROF_ROWS) : -1;
+    k_rows<<<rows_blocks(eng, warps * 32, per_warp * warps), warps * 32, per_warp * warps, st>>>(
+        d_ctx, nctx, G, split, rwm);
+    prof_end(pe);
+    k_ctrl<<<nctx, 128, 0, st>>>(d_ctx, nctx, CTRL_DP_ROWS);
+    pe = prof ? prof_begin(PROF_GROW) : -1;
+    k_grow<<<eng->grow_blocks, 256, 0, st>>>(d_ctx, nctx, G, split);
+    prof_end(pe);
+    k_ctrl<<<nctx, 128, 0, st>>>(d_ctx, nctx, CTRL_DP_GROW);
+  }
+
+  // The level loop as a CUDA graph: a WHILE node whose body is one level plus a
+  // kernel that decides whether to go on (no query finished, iterations left).
+  gst_status loop_graph(int rwm, cudaGraphExec_t* out) {
+    for (auto& lg : graphs)
+      if (lg.nctx == nctx && lg.rw_max == rwm) {
+        *out = lg.exec;
+        return GST_OK;
+      }
+    LoopGraph lg;
+    lg.nctx = nctx;
+    lg.rw_max = rwm;
+    CK(cudaGraphCreate(&lg.graph, 0));
+    cudaGraphConditionalHandle handle;
+    CK(cudaGraphConditionalHandleCreate(&handle, lg.graph, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = handle;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    CK(cudaGraphAddNode(&node, lg.graph, nullptr, 0, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    {
+      // occupancy queries before the capture
+      const int warps = std::max(1, eng->cfg.threads_per_block / 32);
+      rows_blocks(eng, warps * 32, rows_smem_per_warp(rwm) * warps);
+    }
+    cudaStream_t cap;
+    CK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    CK(cudaStreamBeginCaptureToGraph(cap, body, nullptr, nullptr, 0,
+                                     cudaStreamCaptureModeThreadLocal));
+    launch_level(cap, rwm, true, false);
+    k_loop_cond<<<1, 64, 0, cap>>>(d_ctx, nctx, d_loop, handle);
+    cudaGraph_t captured = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(cap, &captured);
+    cudaStreamDestroy(cap);
+    if (ce != cudaSuccess) {
+      cudaGraphDestroy(lg.graph);
+      return fail(eng, GST_DEVICE_ERROR, std::string("graph capture: ") + cudaGetErrorString(ce));
+    }
+    CK(cudaGraphInstantiate(&lg.exec, lg.graph, 0));
+    graphs.push_back(lg);
+    *out = lg.exec;
+    return GST_OK;
+  }
+
+  // Run levels until at least one resident query has finished (or, with
+  // max_levels > 0, at most about that many levels), then read the contexts.
+  gst_status run(int max_levels) {
+    {
+      gst_status s = write_idle();
+      if (s != GST_OK) return s;
+    }
+    const int rwm = rw_max();
+    bool any_sssp = true;
+    const bool prof = eng->cfg.profile_kernels != 0;
+    const bool graphs_on = eng->cfg.use_graphs && !prof;
+    for (;;) {
+      int levels = 0;
+      if (graphs_on) {
+        cudaGraphExec_t ex;
+        gst_status s = loop_graph(rwm, &ex);
+        if (s != GST_OK) return s;
+        const uint32_t iters = max_levels > 0 ? (uint32_t)max_levels : 4096u;
+        loop_init[0] = iters;
+        loop_init[1] = 0u;
+        CK(cudaMemcpyAsync(d_loop, loop_init, 2 * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                           eng->stream));
+        CK(cudaGraphLaunch(ex, eng->stream));
+        CK(cudaMemcpyAsync(loop_left, d_loop, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                           eng->stream));
+        levels = (int)iters;
+      } else {
+        const int ahead = 6;
+        for (int i = 0; i < ahead; i++) launch_level(eng->stream, rwm, any_sssp, prof);
+        cs.launches += (int64_t)ahead * (any_sssp ? 6 : 4);
+        levels = ahead;
+      }
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(h_ctx, d_ctx, sizeof(Ctx) * nctx, cudaMemcpyDeviceToHost, eng->stream));
+      cs.d2h += (int64_t)sizeof(Ctx) * nctx;
+      CK(cudaStreamSynchronize(eng->stream));
+      if (graphs_on) {
+        // levels the device loop ran: each is 7 kernels (sssp, rows, grow, 3 ctrl, loop test)
+        const int64_t ran = (int64_t)levels - (int64_t)loop_left[0];
+        cs.launches += 7 * ran;
+        cs.graph_launches++;
+        cs.graph_levels += ran;
+        levels = (int)ran;
+      }
+      bool any_done = false;
+      any_sssp = false;
+      for (int s = 0; s < nctx; s++) {
+        if (!owner[s]) continue;
+        any_sssp |= h_ctx[s].phase == PH_SSSP || h_ctx[s].phase == PH_PREP;
+        any_done |= h_ctx[s].phase >= PH_DONE;
+        if (eng->cfg.verbose > 1)
+          fprintf(stderr, "[gst run] slot %d k %d phase %u levels %u err %x ub %u n_rows %u in_n %u\n",
+                  s, h_ctx[s].k, h_ctx[s].phase, h_ctx[s].levels, h_ctx[s].error, h_ctx[s].ub,
+                  h_ctx[s].n_rows, h_ctx[s].in_n);
+      }
+      if (any_done || active == 0) return GST_OK;
+      if (max_levels > 0 && levels >= max_levels) return GST_OK;
+    }
+  }
+
+  // Extract the trees of finished queries, fill their results and free their
+  // slots; finished jobs are appended to `done` (capacity overflows are returned
+  // in `retry` with a larger worklist boost instead, unless already at the worst case).
+  gst_status harvest(std::vector<Job*>& done, std::vector<Job*>& retry) {
+    bool any = false;
+    for (int s = 0; s < nctx; s++) any |= owner[s] && h_ctx[s].phase >= PH_DONE;
+    if (!any) return GST_OK;
+    const DevGraph G = dev_graph(g);
+    k_extract<<<1, MAXB, 0, eng->stream>>>(d_ctx, nctx, G);
+    cs.launches += 1;
+    CK(cudaMemcpyAsync(h_ctx, d_ctx, sizeof(Ctx) * nctx, cudaMemcpyDeviceToHost, eng->stream));
+    cs.d2h += (int64_t)sizeof(Ctx) * nctx;
+    CK(cudaStreamSynchronize(eng->stream));
+    std::vector<int32_t> raw;
+    for (int s = 0; s < nctx; s++) {
+      Job* j = owner[s];
+      if (!j || h_ctx[s].phase < PH_DONE) continue;
+      const Ctx c = h_ctx[s];
+      owner[s] = nullptr;
+      active--;
+      if ((c.error & (ERR_QCAP | ERR_FARCAP)) &&
+          !cap_is_worst(g->V, g->E, j->rw, eng->cfg.split_degree, c.qcap)) {
+        j->boost++;
+        retry.push_back(j);
+        continue;
+      }
+      const uint32_t nout = std::min(c.n_out, mem[s].outcap);
+      raw.resize((size_t)nout * 3);
+      if (nout) {
+        CK(cudaMemcpyAsync(raw.data(), mem[s].out, (size_t)nout * 12, cudaMemcpyDeviceToHost,
+                           eng->stream));
+        cs.d2h += (int64_t)nout * 12;
+        CK(cudaStreamSynchronize(eng->stream));
+      }
+      fill(c, j, raw, nout);
+      if (c.error || c.phase != PH_DONE) {
+        char msg[160];
+        snprintf(msg, sizeof msg, "query tag %llu: phase %u error bits 0x%x bounds site %u levels %u",
+                 (unsigned long long)j->q.user_tag, c.phase, c.error, c.bad_site, c.levels);
+        fail(eng, (gst_status)j->out->status, msg);
+      }
+      j->done = true;
+      done.push_back(j);
+    }
+    // idle contexts for the slots just freed
+    return write_idle();
+  }
+
+  static void fill(const Ctx& c, Job* j, const std::vector<int32_t>& raw, uint32_t nout) {
+    gst_result* r = j->out;
+    memset(r, 0, sizeof(*r));
+    r->user_tag = j->q.user_tag;
+    r->status = status_of(c);
+    if (c.error & ERR_EXTRACT) r->status = GST_DEVICE_ERROR;
+    r->stats.levels = c.levels;
+    r->stats.states_expanded = (int64_t)c.st_items;
+    r->stats.edge_relaxations = (int64_t)c.st_relax;
+    r->stats.merge_pairs = (int64_t)c.st_merge;
+    r->stats.rows_merged = (int64_t)c.st_rows;
+    r->stats.sssp_relaxations = (int64_t)c.st_sssp;
+    r->stats.queue_max = c.st_qmax;
+    r->stats.latency_ms =
+        std::chrono::duration<double, std::milli>(Clock::now() - j->t_submit).count();
+    if (r->status != GST_OK) return;
+    r->cost = (int32_t)(c.best >> 32);
+    r->root = (int32_t)(c.best & 0x7FFFFFFull);
+    r->root_hop = (int32_t)((c.best >> 27) & 31u);
+    // distinct edges, (min, max) orientation
+    std::vector<std::pair<std::pair<int32_t, int32_t>, int32_t>> es;
+    es.reserve(nout);
+    for (size_t i = 0; i < nout; i++) {
+      int32_t a = raw[3 * i], b = raw[3 * i + 1];
+      if (a > b) std::swap(a, b);
+      es.push_back({{a, b}, raw[3 * i + 2]});
+    }
+    std::sort(es.begin(), es.end());
+    es.erase(std::unique(es.begin(), es.end(),
+                         [](const auto& x, const auto& y) { return x.first == y.first; }),
+             es.end());
+    r->n_edges = (int64_t)es.size();
+    if (!es.empty()) {
+      r->edge_u = (int32_t*)malloc(sizeof(int32_t) * es.size());
+      r->edge_v = (int32_t*)malloc(sizeof(int32_t) * es.size());
+      r->edge_w = (int32_t*)malloc(sizeof(int32_t) * es.size());
+      for (size_t i = 0; i < es.size(); i++) {
+        r->edge_u[i] = es[i].first.first;
+        r->edge_v[i] = es[i].first.second;
+        r->edge_w[i] = es[i].second;
+      }
+    }
+  }
+
+  // Summed profiled kernel time of this call (grow, rows, sssp), in ms.
+  void kernel_ms(double out[3]) {
+    out[0] = out[1] = out[2] = 0;
+    for (auto& pr : cs.prof) {
+      float e = 0;
+      if (cudaEventElapsedTime(&e, eng->prof_events[2 * pr.second],
+                               eng->prof_events[2 * pr.second + 1]) == cudaSuccess)
+        out[pr.first] += e;
+    }
+  }
+};
+
+// Fill job j from query q (copying the group ids) with result destination r.
+void make_job(Job& j, const gst_query* q, gst_result* r) {
+  j.q = *q;
+  for (int i = 0; i < q->k && i < KMAX; i++) j.gids[i] = q->group_ids[i];
+  j.q.group_ids = j.gids;
+  j.out = r;
+  j.t_submit = Clock::now();
+  j.rw = row_width(q->k, q->hop_bound);
+}
+
+}  // namespace
+
+// ---- serving -------------------------------------------------------------------
+struct gst_server {
+  gst_graph* g = nullptr;
+  gst_groups* grp = nullptr;
+  std::unique_ptr<Runner> run;
+  std::thread th;
+  std::mutex mu;                       // guards everything below
+  std::condition_variable cv_work;     // submissions / stop
+  std::condition_variable cv_done;     // completions
+  std::deque<Job*> pending;
+  std::map<uint64_t, std::unique_ptr<Job>> jobs;        // ticket -> job (owns the result)
+  std::map<uint64_t, std::unique_ptr<gst_result>> res;  // ticket -> result storage
+  uint64_t next_ticket = 1;
+  bool stop = false;
+  gst_status fatal = GST_OK;
+  std::string fatal_msg;
+  int64_t admitted = 0, completed = 0;
+};
+
+namespace {
+
+void server_loop(gst_server* sv) {
+  gst_engine* eng = sv->g->eng;
+  Runner& R = *sv->run;
+  std::vector<Job*> done, retry;
+  for (;;) {
+    // admit what fits, in arrival order (a query that must wait blocks the ones
+    // behind it, so that a large query is not starved by small ones)
+    {
+      std::unique_lock<std::mutex> lk(sv->mu);
+      if (R.active == 0)
+        sv->cv_work.wait(lk, [&] { return sv->stop || !sv->pending.empty(); });
+      if (eng->cfg.verbose)
+        fprintf(stderr, "[gst server] top: stop %d active %d pending %zu\n", (int)sv->stop,
+                R.active, sv->pending.size());
+      if (sv->stop && sv->pending.empty() && R.active == 0) return;
+    }
+    done.clear();
+    retry.clear();
+    {
+      std::lock_guard<std::mutex> elk(eng->mu);
+      cudaSetDevice(eng->device);
+      for (;;) {
+        Job* j = nullptr;
+        {
+          std::lock_guard<std::mutex> lk(sv->mu);
+          if (sv->pending.empty()) break;
+          j = sv->pending.front();
+        }
+        gst_status s = R.admit(j);
+        if (s == GST_NOT_READY) break;
+        std::lock_guard<std::mutex> lk(sv->mu);
+        sv->pending.pop_front();
+        if (s == GST_OK) {
+          sv->admitted++;
+          continue;
+        }
+        memset(j->out, 0, sizeof(gst_result));
+        j->out->status = s;
+        j->out->user_tag = j->q.user_tag;
+        j->done = true;
+        sv->completed++;
+        sv->cv_done.notify_all();
+      }
+      bool waiting;
+      {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        waiting = !sv->pending.empty();
+      }
+      gst_status s = GST_OK;
+      if (eng->cfg.verbose) {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        fprintf(stderr, "[gst server] active %d pending %zu held %zu budget %zu\n", R.active,
+                sv->pending.size(), R.held, R.budget);
+      }
+      if (R.active > 0) {
+        // with arrivals waiting for a slot, come back at the next finished query;
+        // with free slots and arrivals possible, check every few levels
+        const bool free_slot = R.active < R.max_slots;
+        s = R.run(waiting || !free_slot ? 0 : 8);
+        if (s == GST_OK) s = R.harvest(done, retry);
+      }
+      std::lock_guard<std::mutex> lk(sv->mu);
+      if (s != GST_OK) {
+        sv->fatal = s;
+        sv->fatal_msg = eng->err;
+        for (int i = 0; i < R.max_slots; i++)
+          if (R.owner[i]) {
+            R.owner[i]->out->status = s;
+            R.owner[i]->done = true;
+            R.owner[i] = nullptr;
+          }
+        for (Job* j : sv->pending) {
+          j->out->status = s;
+          j->done = true;
+        }
+        sv->pending.clear();
+        R.active = 0;
+        sv->cv_done.notify_all();
+        return;
+      }
+      for (Job* j : retry) sv->pending.push_front(j);
+      sv->completed += (int64_t)done.size();
+      if (!done.empty()) sv->cv_done.notify_all();
     }
   }
 }
@@ -351,9 +826,9 @@ void gst_config_default(gst_config* cfg) {
   cfg->bucket_delta = 0;
   cfg->max_levels = 1 << 20;
   cfg->threads_per_block = 256;
-  cfg->blocks_per_sm = 4;
+  cfg->blocks_per_sm = 8;
   cfg->max_batch = 16;
-  cfg->use_graphs = 0;
+  cfg->use_graphs = 1;
   cfg->verbose = 0;
 }
 
@@ -376,7 +851,9 @@ gst_status gst_engine_create(int32_t device, const gst_config* cfg, gst_engine**
     if (eng->cfg.threads_per_block <= 0) eng->cfg.threads_per_block = d.threads_per_block;
     if (eng->cfg.blocks_per_sm <= 0) eng->cfg.blocks_per_sm = d.blocks_per_sm;
     if (eng->cfg.max_batch <= 0) eng->cfg.max_batch = d.max_batch;
+    if (eng->cfg.use_graphs < 0) eng->cfg.use_graphs = 0;
   }
+  eng->cfg.threads_per_block = std::max(32, std::min(1024, eng->cfg.threads_per_block / 32 * 32));
   eng->cfg.max_batch = std::min(eng->cfg.max_batch, MAXB);
   if (cudaSetDevice(device) != cudaSuccess) {
     delete eng;
@@ -385,13 +862,24 @@ gst_status gst_engine_create(int32_t device, const gst_config* cfg, gst_engine**
   cudaDeviceProp prop;
   cudaGetDeviceProperties(&prop, device);
   eng->sms = prop.multiProcessorCount;
-  eng->grow_blocks = eng->sms * eng->cfg.blocks_per_sm;
-  eng->sssp_blocks = eng->sms * eng->cfg.blocks_per_sm;
+  int occ_grow = 1, occ_sssp = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_grow, k_grow, 256, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sssp, k_sssp, 256, 0);
+  eng->grow_blocks = eng->sms * std::max(1, std::min(occ_grow, eng->cfg.blocks_per_sm));
+  eng->sssp_blocks = eng->sms * std::max(1, std::min(occ_sssp, eng->cfg.blocks_per_sm));
+  // a pool of our own, keeping freed slot memory for the next query
+  cudaMemPoolProps pp = {};
+  pp.allocType = cudaMemAllocationTypePinned;
+  pp.location.type = cudaMemLocationTypeDevice;
+  pp.location.id = device;
   if (cudaStreamCreateWithFlags(&eng->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreate(&eng->ev0) != cudaSuccess || cudaEventCreate(&eng->ev1) != cudaSuccess) {
+      cudaMemPoolCreate(&eng->pool, &pp) != cudaSuccess) {
+    if (eng->stream) cudaStreamDestroy(eng->stream);
     delete eng;
-    return fail(nullptr, GST_DEVICE_ERROR, "engine: stream/event creation failed");
+    return fail(nullptr, GST_DEVICE_ERROR, "engine: stream / memory pool creation failed");
   }
+  uint64_t keep = ~0ull;
+  cudaMemPoolSetAttribute(eng->pool, cudaMemPoolAttrReleaseThreshold, &keep);
   cudaFuncSetAttribute(k_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   *out = eng;
   return GST_OK;
@@ -400,10 +888,12 @@ gst_status gst_engine_create(int32_t device, const gst_config* cfg, gst_engine**
 gst_status gst_engine_destroy(gst_engine* eng) {
   if (!eng) return GST_OK;
   cudaSetDevice(eng->device);
-  if (eng->stream) cudaStreamDestroy(eng->stream);
-  if (eng->ev0) cudaEventDestroy(eng->ev0);
-  if (eng->ev1) cudaEventDestroy(eng->ev1);
+  if (eng->stream) {
+    cudaStreamSynchronize(eng->stream);
+    cudaStreamDestroy(eng->stream);
+  }
   for (auto e : eng->prof_events) cudaEventDestroy(e);
+  if (eng->pool) cudaMemPoolDestroy(eng->pool);
   delete eng;
   return GST_OK;
 }
@@ -427,7 +917,7 @@ static gst_status graph_create_impl(gst_engine* eng, int64_t V, int64_t E, const
     if (beg[v + 1] < beg[v]) return fail(eng, GST_BAD_INPUT, "graph: beg_pos not monotone");
   // Two device copies of the adjacency: sorted by neighbour (edge-weight lookups
   // of the tree walk) and sorted by weight, with per vertex the number of edges of
-  // weight <= 2^j (j < WIDX), so that a grow step reads only the edges light enough
+  // weight <= widx_threshold(t) (t < WIDX), so that a grow step reads only the edges light enough
   // to keep its target under the upper bound.
   std::vector<int2> edges((size_t)E), wedges((size_t)E);
   std::vector<uint32_t> widx((size_t)V * WIDX);
@@ -450,7 +940,7 @@ static gst_status graph_create_impl(gst_engine* eng, int64_t V, int64_t E, const
       std::sort(tmp.begin(), tmp.end());
       size_t j = 0;
       for (int t = 0; t < WIDX; t++) {
-        while (j < tmp.size() && tmp[j].first <= (1 << t)) j++;
+        while (j < tmp.size() && (uint32_t)tmp[j].first <= widx_threshold(t)) j++;
         widx[(size_t)v * WIDX + t] = (uint32_t)j;
       }
       for (size_t i = 0; i < tmp.size(); i++)
@@ -465,13 +955,10 @@ static gst_status graph_create_impl(gst_engine* eng, int64_t V, int64_t E, const
   g->eng = eng;
   g->V = V;
   g->E = E;
-  g->h_beg.assign(beg, beg + V + 1);
   CK(cudaMalloc(&g->d_beg, sizeof(int64_t) * (V + 1)));
   CK(cudaMalloc(&g->d_edges, sizeof(int2) * std::max<int64_t>(E, 1)));
   CK(cudaMalloc(&g->d_wedges, sizeof(int2) * std::max<int64_t>(E, 1)));
   CK(cudaMalloc(&g->d_widx, sizeof(uint32_t) * V * WIDX));
-  CK(cudaMalloc(&g->d_ctx, sizeof(Ctx) * MAXB));
-  CK(cudaMallocHost(&g->h_ctx, sizeof(Ctx) * MAXB));
   // stream-ordered copies, completed before returning: the level kernels run on a
   // non-blocking stream that does not wait for the legacy default stream
   CK(cudaMemcpyAsync(g->d_beg, beg, sizeof(int64_t) * (V + 1), cudaMemcpyHostToDevice,
@@ -514,13 +1001,12 @@ gst_status gst_graph_destroy(gst_graph* g) {
   std::lock_guard<std::mutex> lk(eng->mu);
   cudaSetDevice(eng->device);
   cudaStreamSynchronize(eng->stream);
-  for (auto& s : g->slots) free_slot(s);
+  g->batch.reset();
   cudaFree(g->d_beg);
   cudaFree(g->d_edges);
   cudaFree(g->d_wedges);
   cudaFree(g->d_widx);
-  cudaFree(g->d_ctx);
-  cudaFreeHost(g->h_ctx);
+  cudaMemPoolTrimTo(eng->pool, 0);
   delete g;
   return GST_OK;
 }
@@ -557,7 +1043,10 @@ gst_status gst_groups_create(gst_graph* g, int32_t n_groups, const int64_t* grp_
 
 gst_status gst_groups_destroy(gst_groups* gr) {
   if (!gr) return GST_OK;
-  cudaSetDevice(gr->g->eng->device);
+  gst_engine* eng = gr->g->eng;
+  std::lock_guard<std::mutex> lk(eng->mu);
+  cudaSetDevice(eng->device);
+  cudaStreamSynchronize(eng->stream);
   cudaFree(gr->d_ptr);
   cudaFree(gr->d_mem);
   delete gr;
@@ -572,9 +1061,21 @@ gst_status gst_solve_batch(gst_graph* g, gst_groups* grp, int32_t n, const gst_q
   for (int32_t i = 0; i < n; i++) memset(&results[i], 0, sizeof(gst_result));
   std::lock_guard<std::mutex> lk(eng->mu);
   CK(cudaSetDevice(eng->device));
-  const int B = std::max(1, std::min<int>(eng->cfg.max_batch, n));
-  // admission: slots sized for the widest query, bounded by the memory budget
-  size_t rw_max = 1;
+  const int B = std::max(1, std::min<int>(eng->cfg.max_batch, std::max<int32_t>(n, 1)));
+  if (!g->batch || g->batch->max_slots < B) {
+    g->batch.reset(new Runner(eng, g, std::max(B, g->batch ? g->batch->max_slots : 0)));
+    gst_status s = g->batch->init();
+    if (s != GST_OK) {
+      g->batch.reset();
+      return s;
+    }
+  }
+  Runner& R = *g->batch;
+  R.grp = grp;
+  R.cs = CallStats();
+  R.nctx = 0;  // no query is resident between calls
+  std::unique_ptr<Job[]> jobs(new Job[(size_t)std::max<int32_t>(n, 1)]);
+  std::deque<Job*> pending;
   for (int32_t i = 0; i < n; i++) {
     gst_status s = validate_query(eng, grp, &queries[i]);
     if (s != GST_OK) {
@@ -582,151 +1083,71 @@ gst_status gst_solve_batch(gst_graph* g, gst_groups* grp, int32_t n, const gst_q
       results[i].user_tag = queries[i].user_tag;
       continue;
     }
-    rw_max = std::max(rw_max, row_width(queries[i].k, queries[i].hop_bound));
+    make_job(jobs[i], &queries[i], &results[i]);
+    pending.push_back(&jobs[i]);
   }
-  size_t free_b = 0, total_b = 0;
-  CK(cudaMemGetInfo(&free_b, &total_b));
-  size_t held = 0;
-  for (auto& s : g->slots) held += s.bytes;
-  const size_t budget = eng->cfg.mem_budget_bytes > 0 ? (size_t)eng->cfg.mem_budget_bytes
-                                                      : (size_t)((free_b + held) * 0.85);
-  const size_t per = slot_bytes(g->V, rw_max);
-  int nslots = (int)std::min<size_t>((size_t)B, budget / std::max<size_t>(per, 1));
-  if (nslots < 1) {
-    for (int32_t i = 0; i < n; i++)
-      if (results[i].status == 0) {
-        results[i].status = GST_OOM_ADMISSION;
-        results[i].user_tag = queries[i].user_tag;
+  cudaEvent_t ev0, ev1;
+  CK(cudaEventCreate(&ev0));
+  CK(cudaEventCreate(&ev1));
+  CK(cudaEventRecord(ev0, eng->stream));
+  // use at most B slots: admitting beyond max_batch would change the batch size
+  const int saved = R.max_slots;
+  R.max_slots = B;
+  gst_status st = GST_OK;
+  std::vector<Job*> done, retry;
+  while (st == GST_OK && (!pending.empty() || R.active > 0)) {
+    while (!pending.empty()) {
+      gst_status s = R.admit(pending.front());
+      if (s == GST_NOT_READY) break;
+      if (s == GST_OOM_ADMISSION) {
+        Job* j = pending.front();
+        j->out->status = GST_OOM_ADMISSION;
+        j->out->user_tag = j->q.user_tag;
+        fail(eng, GST_OOM_ADMISSION, "solve: the query's state table does not fit the memory budget");
+      } else if (s != GST_OK) {
+        st = s;
+        break;
       }
-    return fail(eng, GST_OOM_ADMISSION, "solve: state table does not fit the memory budget");
-  }
-  for (int s = 0; s < nslots; s++) {
-    gst_status st = ensure_slot(eng, g, (size_t)s, rw_max);
-    if (st != GST_OK) return st;
-  }
-  // slot -> query index; -1 = free
-  std::vector<int> owner(nslots, -1);
-  std::vector<int32_t> raw((size_t)(1 << 16) * 3);
-  int32_t next = 0;
-  auto next_valid = [&]() {
-    while (next < n && results[next].status != 0) next++;
-    return next < n ? next++ : -1;
-  };
-  eng->cs = CallStats();
-  const auto t_call = std::chrono::steady_clock::now();
-  std::vector<double> lat(n > 0 ? n : 1, 0.0);
-  CK(cudaEventRecord(eng->ev0, eng->stream));
-  int active = 0;
-  // fill and run in waves of refills: a finished slot is refilled at the next check
-  for (;;) {
-    for (int s = 0; s < nslots; s++) {
-      if (owner[s] >= 0) continue;
-      int qi = next_valid();
-      if (qi < 0) break;
-      const gst_query* q = &queries[qi];
-      Slot& sl = g->slots[s];
-      Ctx& hc = g->h_ctx[s];
-      prep_ctx(eng, g, sl, q, hc);
-      gst_status st = reset_slot(eng, g, sl, (size_t)hc.RW, hc.use_lb != 0);
-      if (st != GST_OK) return st;
-      CK(cudaMemcpyAsync(g->d_ctx + s, &hc, sizeof(Ctx), cudaMemcpyHostToDevice, eng->stream));
-      eng->cs.h2d += sizeof(Ctx);
-      eng->cs.launches += 2;
-      // k_init for this slot alone: grid.y selects the context
-      const DevGraph G = dev_graph(g);
-      k_init<<<dim3(64, 1), 256, 0, eng->stream>>>(g->d_ctx + s, 1, G, grp->d_ptr, grp->d_mem,
-                                                   eng->cfg.split_degree);
-      k_ctrl<<<1, 32, 0, eng->stream>>>(g->d_ctx + s, 1, CTRL_SSSP);
-      owner[s] = qi;
-      active++;
+      pending.pop_front();
     }
-    if (active == 0) break;
-    // contexts of free slots must look finished to the level kernels
-    for (int s = 0; s < nslots; s++)
-      if (owner[s] < 0) {
-        Ctx& idle = g->h_ctx[s];
-        memset(&idle, 0, sizeof(idle));
-        idle.phase = PH_DONE;
-        idle.best = ~0ull;
-        CK(cudaMemcpyAsync(g->d_ctx + s, &idle, sizeof(Ctx), cudaMemcpyHostToDevice, eng->stream));
-        eng->cs.h2d += sizeof(Ctx);
-      }
-    LoopShape sh;
-    sh.sssp = true;
-    sh.rw_max = (int)rw_max;
-    // run until at least one query finishes
-    const int ahead = 6;
-    bool any_done = false;
-    while (!any_done) {
-      for (int i = 0; i < ahead; i++) {
-        gst_status st = launch_level(eng, g, nslots, sh);
-        if (st != GST_OK) return st;
-      }
-      CK(cudaMemcpyAsync(g->h_ctx, g->d_ctx, sizeof(Ctx) * nslots, cudaMemcpyDeviceToHost,
-                         eng->stream));
-      eng->cs.d2h += (int64_t)sizeof(Ctx) * nslots;
-      CK(cudaStreamSynchronize(eng->stream));
-      bool any_sssp = false;
-      for (int s = 0; s < nslots; s++) {
-        if (owner[s] < 0) continue;
-        any_sssp |= g->h_ctx[s].phase == PH_SSSP || g->h_ctx[s].phase == PH_PREP;
-        any_done |= g->h_ctx[s].phase >= PH_DONE;
-      }
-      sh.sssp = any_sssp;
-    }
-    // harvest finished queries
-    const DevGraph G = dev_graph(g);
-    k_extract<<<1, MAXB, 0, eng->stream>>>(g->d_ctx, nslots, G);
-    eng->cs.launches += 1;
-    CK(cudaMemcpyAsync(g->h_ctx, g->d_ctx, sizeof(Ctx) * nslots, cudaMemcpyDeviceToHost,
-                       eng->stream));
-    eng->cs.d2h += (int64_t)sizeof(Ctx) * nslots;
-    CK(cudaStreamSynchronize(eng->stream));
-    for (int s = 0; s < nslots; s++) {
-      if (owner[s] < 0 || g->h_ctx[s].phase < PH_DONE) continue;
-      const Ctx c = g->h_ctx[s];
-      const uint32_t nout = std::min(c.n_out, g->slots[s].outcap);
-      if (nout) {
-        CK(cudaMemcpyAsync(raw.data(), g->slots[s].out, (size_t)nout * 12,
-                           cudaMemcpyDeviceToHost, eng->stream));
-        eng->cs.d2h += (int64_t)nout * 12;
-        CK(cudaStreamSynchronize(eng->stream));
-      }
-      fill_result(g, c, &queries[owner[s]], raw, &results[owner[s]]);
-      if (c.error || c.phase != PH_DONE) {
-        char msg[160];
-        snprintf(msg, sizeof msg, "query %d: phase %u error bits 0x%x bounds site %u levels %u",
-                 owner[s], c.phase, c.error, c.bad_site, c.levels);
-        fail(eng, (gst_status)results[owner[s]].status, msg);
-      }
-      if (c.error & ERR_EXTRACT) results[owner[s]].status = GST_DEVICE_ERROR;
-      lat[owner[s]] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() -
-                                                               t_call).count();
-      owner[s] = -1;
-      active--;
-    }
+    if (st != GST_OK || R.active == 0) break;
+    st = R.run(0);
+    done.clear();
+    retry.clear();
+    if (st == GST_OK) st = R.harvest(done, retry);
+    for (Job* j : retry) pending.push_front(j);
   }
-  CK(cudaEventRecord(eng->ev1, eng->stream));
-  CK(cudaEventSynchronize(eng->ev1));
+  R.max_slots = saved;
+  CK(cudaEventRecord(ev1, eng->stream));
+  CK(cudaEventSynchronize(ev1));
   float ms = 0;
-  cudaEventElapsedTime(&ms, eng->ev0, eng->ev1);
-  double kms[3] = {0, 0, 0};
-  for (auto& pr : eng->cs.prof) {
-    float e = 0;
-    if (cudaEventElapsedTime(&e, eng->prof_events[2 * pr.second],
-                             eng->prof_events[2 * pr.second + 1]) == cudaSuccess)
-      kms[pr.first] += e;
+  cudaEventElapsedTime(&ms, ev0, ev1);
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
+  if (st != GST_OK) {
+    // a device failure ends the call; the runner is rebuilt on the next call
+    std::string msg = eng->err;
+    g->batch.reset();
+    cudaGetLastError();
+    for (int32_t i = 0; i < n; i++)
+      if (!jobs[i].done && results[i].status == GST_OK) results[i].status = st;
+    return fail(eng, st, msg);
   }
+  if (eng->cfg.verbose)
+    fprintf(stderr, "[gst batch] %d queries: %.3f ms, %lld launches, %lld graph launches, %lld graph levels\n",
+            n, ms, (long long)R.cs.launches, (long long)R.cs.graph_launches,
+            (long long)R.cs.graph_levels);
+  double kms[3];
+  R.kernel_ms(kms);
   for (int32_t i = 0; i < n; i++) {
-    gst_stats& st = results[i].stats;
-    st.device_ms = ms;
-    st.latency_ms = lat[i];
-    st.kernel_launches = eng->cs.launches;
-    st.h2d_bytes = eng->cs.h2d;
-    st.d2h_bytes = eng->cs.d2h;
-    st.grow_ms = kms[PROF_GROW];
-    st.rows_ms = kms[PROF_ROWS];
-    st.sssp_ms = kms[PROF_SSSP];
+    gst_stats& s = results[i].stats;
+    s.device_ms = ms;
+    s.kernel_launches = R.cs.launches;
+    s.h2d_bytes = R.cs.h2d;
+    s.d2h_bytes = R.cs.d2h;
+    s.grow_ms = kms[PROF_GROW];
+    s.rows_ms = kms[PROF_ROWS];
+    s.sssp_ms = kms[PROF_SSSP];
   }
   return GST_OK;
 }
@@ -741,10 +1162,17 @@ gst_status gst_solve(gst_graph* g, gst_groups* grp, const gst_query* q, gst_resu
     res->user_tag = q->user_tag;
     return s;
   }
-  const int32_t saved = eng->cfg.max_batch;
-  eng->cfg.max_batch = 1;
+  int32_t saved;
+  {
+    std::lock_guard<std::mutex> lk(eng->mu);
+    saved = eng->cfg.max_batch;
+    eng->cfg.max_batch = 1;
+  }
   s = gst_solve_batch(g, grp, 1, q, res);
-  eng->cfg.max_batch = saved;
+  {
+    std::lock_guard<std::mutex> lk(eng->mu);
+    eng->cfg.max_batch = saved;
+  }
   if (s != GST_OK) return s;
   return (gst_status)res->status;
 }
@@ -752,19 +1180,21 @@ gst_status gst_solve(gst_graph* g, gst_groups* grp, const gst_query* q, gst_resu
 gst_status gst_debug_slot_state(gst_graph* g, int32_t slot, uint64_t* cells, int64_t n_cells,
                                 uint64_t* best_out) {
   gst_engine* eng = g ? g->eng : nullptr;
-  if (!g || slot < 0 || (size_t)slot >= g->slots.size() || n_cells < 0)
+  if (!g || !g->batch || slot < 0 || slot >= g->batch->max_slots || n_cells < 0 ||
+      !g->batch->mem[slot].base)
     return fail(eng, GST_BAD_INPUT, "debug: bad slot");
   std::lock_guard<std::mutex> lk(eng->mu);
   CK(cudaSetDevice(eng->device));
-  const Slot& s = g->slots[slot];
-  const int64_t have = (int64_t)(s.V * s.rw_cap);
+  Runner& R = *g->batch;
+  const SlotMem& m = R.mem[slot];
+  const int64_t have = (int64_t)(g->V * (int64_t)m.rw);
   if (cells && n_cells)
-    CK(cudaMemcpyAsync(cells, s.table, (size_t)std::min(n_cells, have) * 8,
+    CK(cudaMemcpyAsync(cells, m.table, (size_t)std::min(n_cells, have) * 8,
                        cudaMemcpyDeviceToHost, eng->stream));
-  CK(cudaMemcpyAsync(g->h_ctx + slot, g->d_ctx + slot, sizeof(Ctx), cudaMemcpyDeviceToHost,
+  CK(cudaMemcpyAsync(R.h_ctx + slot, R.d_ctx + slot, sizeof(Ctx), cudaMemcpyDeviceToHost,
                      eng->stream));
   CK(cudaStreamSynchronize(eng->stream));
-  if (best_out) *best_out = g->h_ctx[slot].best;
+  if (best_out) *best_out = R.h_ctx[slot].best;
   return GST_OK;
 }
 
@@ -775,6 +1205,106 @@ void gst_result_free(gst_result* r) {
   free(r->edge_w);
   r->edge_u = r->edge_v = r->edge_w = nullptr;
   r->n_edges = 0;
+}
+
+// ---- serving ---------------------------------------------------------------------
+
+gst_status gst_server_create(gst_graph* g, gst_groups* grp, gst_server** out) {
+  gst_engine* eng = g ? g->eng : nullptr;
+  if (!g || !grp || grp->g != g || !out) return fail(eng, GST_BAD_INPUT, "server: bad arguments");
+  *out = nullptr;
+  gst_server* sv = new gst_server();
+  sv->g = g;
+  sv->grp = grp;
+  {
+    std::lock_guard<std::mutex> lk(eng->mu);
+    CK(cudaSetDevice(eng->device));
+    sv->run.reset(new Runner(eng, g, std::max(1, eng->cfg.max_batch)));
+    sv->run->grp = grp;
+    gst_status s = sv->run->init();
+    if (s != GST_OK) {
+      delete sv;
+      return s;
+    }
+  }
+  sv->th = std::thread(server_loop, sv);
+  *out = sv;
+  return GST_OK;
+}
+
+gst_status gst_submit(gst_server* sv, const gst_query* q, uint64_t* ticket) {
+  if (!sv || !q || !ticket) return fail(nullptr, GST_BAD_INPUT, "submit: bad arguments");
+  gst_engine* eng = sv->g->eng;
+  std::unique_ptr<Job> j(new Job());
+  std::unique_ptr<gst_result> r(new gst_result());
+  memset(r.get(), 0, sizeof(gst_result));
+  gst_status s = validate_query(eng, sv->grp, q);
+  std::lock_guard<std::mutex> lk(sv->mu);
+  if (sv->fatal != GST_OK) return fail(eng, sv->fatal, "submit: server stopped: " + sv->fatal_msg);
+  if (sv->stop) return fail(eng, GST_BAD_INPUT, "submit: server is shutting down");
+  const uint64_t t = sv->next_ticket++;
+  if (s == GST_OK) make_job(*j, q, r.get());
+  j->ticket = t;
+  j->out = r.get();
+  if (s != GST_OK) {
+    r->status = s;
+    r->user_tag = q->user_tag;
+    j->done = true;
+  }
+  Job* raw = j.get();
+  sv->jobs[t] = std::move(j);
+  sv->res[t] = std::move(r);
+  if (s == GST_OK) {
+    sv->pending.push_back(raw);
+    sv->cv_work.notify_one();
+  }
+  *ticket = t;
+  return GST_OK;
+}
+
+static gst_status take_result(gst_server* sv, uint64_t ticket, gst_result* res) {
+  auto it = sv->jobs.find(ticket);
+  *res = *sv->res[ticket];  // ownership of the edge arrays moves to the caller
+  sv->jobs.erase(it);
+  sv->res.erase(ticket);
+  return (gst_status)res->status;
+}
+
+gst_status gst_poll(gst_server* sv, uint64_t ticket, gst_result* res) {
+  if (!sv || !res) return fail(nullptr, GST_BAD_INPUT, "poll: bad arguments");
+  std::lock_guard<std::mutex> lk(sv->mu);
+  auto it = sv->jobs.find(ticket);
+  if (it == sv->jobs.end()) return fail(sv->g->eng, GST_BAD_INPUT, "poll: unknown ticket");
+  if (!it->second->done) return GST_NOT_READY;
+  return take_result(sv, ticket, res);
+}
+
+gst_status gst_wait(gst_server* sv, uint64_t ticket, gst_result* res) {
+  if (!sv || !res) return fail(nullptr, GST_BAD_INPUT, "wait: bad arguments");
+  std::unique_lock<std::mutex> lk(sv->mu);
+  auto it = sv->jobs.find(ticket);
+  if (it == sv->jobs.end()) return fail(sv->g->eng, GST_BAD_INPUT, "wait: unknown ticket");
+  Job* j = it->second.get();
+  sv->cv_done.wait(lk, [&] { return j->done.load(); });
+  return take_result(sv, ticket, res);
+}
+
+gst_status gst_server_destroy(gst_server* sv) {
+  if (!sv) return GST_OK;
+  {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    sv->stop = true;
+    sv->cv_work.notify_all();
+  }
+  if (sv->th.joinable()) sv->th.join();
+  {
+    gst_engine* eng = sv->g->eng;
+    std::lock_guard<std::mutex> lk(eng->mu);
+    sv->run.reset();
+  }
+  for (auto& kv : sv->res) gst_result_free(kv.second.get());
+  delete sv;
+  return GST_OK;
 }
 
 }  // extern "C"
@@ -810,7 +1340,6 @@ constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mu;
 void* g_noalloc_ptr[kMaxDevices] = {nullptr};
 
-size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 // Device address of the scratch array on `device` (must be current).  Host code
 // cannot use the symbol itself: on the host it names a stand-in object, not
@@ -958,6 +1487,7 @@ gst_status noalloc_solve(int device, cudaStream_t st, int64_t V, int64_t E, cons
   c.far_min = 0xFFFFFFFFu;
   c.bucket_end = 0xFFFFFFFFu;
   c.ub = 0xFFFFFFFFu;
+  c.cut = 0xFFFFFFFFu;
   c.ub_cell = 0xFFFFFFFFu;
   c.best = ~0ull;
   c.phase = c.use_lb ? PH_SSSP : PH_DP;

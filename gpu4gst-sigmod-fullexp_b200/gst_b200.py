@@ -285,7 +285,8 @@ class Stats(C.Structure):
                 ("rows_merged", C.c_int64), ("sssp_relaxations", C.c_int64),
                 ("kernel_launches", C.c_int64), ("h2d_bytes", C.c_int64),
                 ("d2h_bytes", C.c_int64), ("device_ms", C.c_double), ("latency_ms", C.c_double),
-                ("grow_ms", C.c_double), ("rows_ms", C.c_double), ("sssp_ms", C.c_double)]
+                ("grow_ms", C.c_double), ("rows_ms", C.c_double), ("sssp_ms", C.c_double),
+                ("queue_max", C.c_int64)]
 
 
 class Result(C.Structure):
@@ -309,11 +310,18 @@ _sig("gst_groups_destroy", C.c_int, [_vp])
 _sig("gst_solve", C.c_int, [_vp, _vp, C.POINTER(Query), C.POINTER(Result)])
 _sig("gst_solve_batch", C.c_int, [_vp, _vp, C.c_int32, C.POINTER(Query), C.POINTER(Result)])
 _sig("gst_result_free", None, [C.POINTER(Result)])
+_sig("gst_server_create", C.c_int, [_vp, _vp, C.POINTER(_vp)])
+_sig("gst_submit", C.c_int, [_vp, C.POINTER(Query), C.POINTER(C.c_uint64)])
+_sig("gst_poll", C.c_int, [_vp, C.c_uint64, C.POINTER(Result)])
+_sig("gst_wait", C.c_int, [_vp, C.c_uint64, C.POINTER(Result)])
+_sig("gst_server_destroy", C.c_int, [_vp])
 
 C_ABI_SYMBOLS = [
     "gst_config_default", "gst_engine_create", "gst_engine_destroy", "gst_last_error_string",
     "gst_graph_create", "gst_graph_create_i64", "gst_graph_destroy", "gst_groups_create",
     "gst_groups_destroy", "gst_solve", "gst_solve_batch", "gst_result_free",
+    "gst_server_create", "gst_submit", "gst_poll", "gst_wait", "gst_server_destroy",
+    "gst_debug_slot_state", "gst_solve_noalloc",
 ]
 
 
@@ -444,3 +452,55 @@ class DeviceGraph:
         if rc != OK:
             raise GstError(f"gst_solve_batch: {STATUS.get(rc, rc)}: {self.eng.error()}")
         return [_answer(rs[i]) for i in range(n)]
+
+    def server(self) -> "Server":
+        return Server(self)
+
+
+class Server:
+    """Continuous-batching server over a resident graph (include/gst.h:
+    gst_server_create / gst_submit / gst_poll / gst_wait).  Queries are admitted
+    into free slots at DP-level boundaries while others run on the GPU."""
+
+    def __init__(self, dg: DeviceGraph):
+        self.dg = dg
+        self._h = _vp()
+        rc = _lib.gst_server_create(dg._g, dg._grp, C.byref(self._h))
+        if rc:
+            raise GstError(f"gst_server_create: {STATUS.get(rc, rc)}: {dg.eng.error()}")
+
+    def submit(self, group_ids, hop_bound: int | None = None, tag: int = 0) -> int:
+        a = np.ascontiguousarray(group_ids, dtype=np.int32)
+        q = Query(len(a), a.ctypes.data_as(C.POINTER(C.c_int32)),
+                  -1 if hop_bound is None else int(hop_bound), tag)
+        t = C.c_uint64(0)
+        rc = _lib.gst_submit(self._h, C.byref(q), C.byref(t))
+        if rc:
+            raise GstError(f"gst_submit: {STATUS.get(rc, rc)}: {self.dg.eng.error()}")
+        return int(t.value)
+
+    def poll(self, ticket: int):
+        """The Answer, or None while the query runs."""
+        r = Result()
+        rc = _lib.gst_poll(self._h, ticket, C.byref(r))
+        if rc == NOT_READY:
+            return None
+        if rc == BAD_INPUT and r.status == 0:
+            raise GstError(f"gst_poll: {self.dg.eng.error()}")
+        return _answer(r)
+
+    def wait(self, ticket: int) -> Answer:
+        r = Result()
+        _lib.gst_wait(self._h, ticket, C.byref(r))
+        return _answer(r)
+
+    def close(self):
+        if self._h:
+            _lib.gst_server_destroy(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -52,6 +52,7 @@ typedef enum gst_status {
 typedef struct gst_engine gst_engine;
 typedef struct gst_graph gst_graph;
 typedef struct gst_groups gst_groups;
+typedef struct gst_server gst_server;
 
 /* Engine tunables; zero fields take defaults (gst_config_default). */
 typedef struct gst_config {
@@ -62,7 +63,9 @@ typedef struct gst_config {
   int32_t threads_per_block;  /* CTA size of the level kernels */
   int32_t blocks_per_sm;      /* resident CTAs per SM for the level kernels */
   int32_t max_batch;          /* queries resident at once in gst_solve_batch / serving */
-  int32_t use_graphs;         /* 1: run the level loop as a CUDA graph with a device-side while node */
+  int32_t use_graphs;         /* 1 (default): run the level loop as a CUDA graph whose
+                                 conditional WHILE node repeats the level body on the device
+                                 until a query finishes; ignored while profile_kernels != 0 */
   int32_t profile_kernels;    /* bit0 grow, bit1 rows, bit2 sssp: bracket those launches with
                                  CUDA events and report their summed device time */
   int32_t verbose;
@@ -90,6 +93,7 @@ typedef struct gst_stats {
   double grow_ms;           /* profiled device time of the grow / rows / sssp launches */
   double rows_ms;           /*   (batch totals; 0 unless cfg.profile_kernels selects them) */
   double sssp_ms;
+  int64_t queue_max;        /* largest worklist fill of the query (items) */
 } gst_stats;
 
 typedef struct gst_result {
@@ -136,6 +140,27 @@ gst_status gst_solve_batch(gst_graph* g, gst_groups* grp, int32_t n, const gst_q
                            gst_result* results);
 
 void gst_result_free(gst_result* res);
+
+/* Serving (no counterpart in the reference, whose drivers run a fixed query list;
+ * this replaces the q_start..q_end loop of GSTnonHop.cu:247 / GPUHop.cu:172 for
+ * queries that arrive over time).  A server owns a host thread and a set of query
+ * slots on the engine's device.  Submitted queries wait in arrival order until a
+ * slot and the HBM of their state table (2^k x (D+1) x V x 8 bytes plus worklists,
+ * within cfg.mem_budget_bytes) are free, and are folded into the running batch at
+ * the next DP-level boundary, alongside queries already on the GPU.  Each result is
+ * the same as gst_solve's for that query. */
+gst_status gst_server_create(gst_graph* g, gst_groups* grp, gst_server** out);
+/* Queue one query (copied); *ticket names it in gst_poll / gst_wait.  A malformed
+ * query is accepted and completes at once with GST_BAD_INPUT. */
+gst_status gst_submit(gst_server* s, const gst_query* q, uint64_t* ticket);
+/* GST_NOT_READY while the query runs; otherwise fills *res (release it with
+ * gst_result_free), forgets the ticket and returns the query's status. */
+gst_status gst_poll(gst_server* s, uint64_t ticket, gst_result* res);
+/* Like gst_poll, but blocks until the query has finished. */
+gst_status gst_wait(gst_server* s, uint64_t ticket, gst_result* res);
+/* Finishes every submitted query, then stops the server's thread and frees its
+ * slots.  Results not taken are released. */
+gst_status gst_server_destroy(gst_server* s);
 
 /* Diagnostics (no counterpart in the reference): copy the first n_cells packed
  * state cells (cost<<32 | pending<<31 | parent) of a query slot and the packed

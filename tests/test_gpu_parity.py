@@ -92,3 +92,35 @@ def test_bad_input_is_reported(engine):
     res = dg.solve_batch([[0, 1], [0, 0], [2, 3]])
     assert res[1].status == G.BAD_INPUT and res[0].ok and res[2].ok
     dg.close()
+
+
+@pytest.mark.parametrize("delta", [1, 3, 16])
+def test_cost_buckets_match_reference(delta):
+    """Cost-ordered frontiers (edges relaxed lazily, bucket by bucket) give the same
+    optimum as the unordered frontier and the reference's solvers."""
+    eng = G.Engine(0, bucket_delta=delta, max_batch=8)
+    try:
+        fx = load_golden("rmat3k_k4_k5")
+        g, grp = golden_inputs(fx)
+        dg = eng.graph(g, grp)
+        qs, hops, want = [], [], []
+        for case in fx["cases"]:
+            costs = next(iter(case["ref"].values()))
+            for q, c in zip(case["queries"], costs):
+                qs.append(q)
+                hops.append(case["hop"])
+                want.append(_ref(c))
+        for q, h, a, w in zip(qs, hops, dg.solve_batch(qs, hops), want):
+            _check(g, grp, q, h, a, w)
+        for q, h, w in list(zip(qs, hops, want))[::7]:
+            _check(g, grp, q, h, dg.solve(q, h), w)
+        dg.close()
+        g = G.synth_rmat(2500, 12000, 77)
+        grp = G.synth_groups_zipf(g.V, 100, 1.5, 2, 50, 78)
+        dg = eng.graph(g, grp)
+        for k in (3, 6):
+            for q in G.synth_queries(grp.n_groups, 3, k, 79 + k):
+                _check(g, grp, q, None, dg.solve(q), O.gst_nonhop(g, grp, q)["cost"])
+        dg.close()
+    finally:
+        eng.close()
