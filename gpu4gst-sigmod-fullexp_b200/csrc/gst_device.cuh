@@ -132,8 +132,10 @@ struct Ctx {
   uint32_t far_min;
   uint32_t bucket_end;
   uint32_t ub;          // best feasible cost known (one-label solutions and full cells)
-  uint32_t cut;         // ub when the one-label distances became final: a distance above
-                        // it (or unreached) is only known to exceed it
+  uint32_t cut;         // cutoff when the one-label distances became final: a distance
+                        // above it (or unreached) is only known to exceed it
+  uint32_t cut_mult;    // the distance search stops at cut_mult x ub (hop-bounded queries
+                        // prune against their own, larger, bound and want more of them)
   uint32_t ub_cell;     // best full-state cell
   unsigned long long best;  // cost<<32 | d<<27 | v of the best full-state cell
   uint32_t phase;
@@ -216,6 +218,12 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x) {
 // list under the key cost + weight(next edge), so heavy edges are read only once
 // the frontier has reached their target cost, by which time ub has usually pruned
 // them.  The near list holds items of the current bucket.
+// Distance cutoff of the one-label search: cut_mult x ub, saturating.
+__device__ __forceinline__ uint32_t sssp_cutoff(const Ctx* c) {
+  const uint64_t x = (uint64_t)__ldcg(&c->ub) * (c->cut_mult ? c->cut_mult : 1u);
+  return x >= COST_INF ? COST_INF : (uint32_t)x;
+}
+
 // Largest edge weight a grow step from a state of cost `cost` can still use: a
 // target must stay <= ub (unbounded) or < ub_cell (hop-bounded).
 __device__ __forceinline__ uint32_t grow_limit(const Ctx* c, uint32_t cost) {
@@ -499,7 +507,7 @@ __global__ void __launch_bounds__(256) k_sssp(Ctx* ctxs, int nctx, DevGraph G, i
         const uint32_t cur = __ldcg(&c->dist[(uint64_t)v * DIST_STRIDE + (gi & ~CHUNK)]);
         // ub is read once per item (a per-edge read of one word by every thread of
         // a one-query launch is an L2 hot spot); a stale, larger ub prunes less
-        ub = __ldcg(&c->ub);
+        ub = sssp_cutoff(c);
         bend = c->bucket_end;
         // not stale, and still able to reach a vertex at distance <= ub
         if (cur >= cost && cost < ub)
@@ -604,7 +612,7 @@ __global__ void __launch_bounds__(256) k_sssp(Ctx* ctxs, int nctx, DevGraph G, i
         }
     }
     best = __reduce_min_sync(0xffffffffu, best);
-    if ((threadIdx.x & 31) == 0 && best < COST_INF && !c->hop && best < __ldcg(&c->ub))
+    if ((threadIdx.x & 31) == 0 && best < COST_INF && best < __ldcg(&c->ub))
       atomicMin(&c->ub, best);
   }
 }
@@ -1050,7 +1058,7 @@ __global__ void k_ctrl(Ctx* ctxs, int nctx, int mode) {
     // The distances are final up to the cutoff ub: every stored distance <= ub is
     // exact, and any other is only known to be > ub.  The group distances feed a
     // lower bound, so they are clamped to ub + 1, a value never above the truth.
-    const uint32_t cut = c->ub;
+    const uint32_t cut = sssp_cutoff(c);
     const uint32_t lim = cut == COST_INF ? COST_INF : cut + 1u;
     for (int i = threadIdx.x; i < KMAX * KMAX; i += blockDim.x) c->vv[i] = min(c->vv[i], lim);
     __syncthreads();

@@ -106,7 +106,7 @@ size_t row_width(int k, int D) { return ((size_t)1 << k) * (size_t)(D >= 0 ? D +
 uint32_t list_cap(int64_t V, int64_t E, size_t rw, int split, int boost) {
   const uint64_t worst = std::min<uint64_t>((uint64_t)V * rw + (uint64_t)E / split * rw + 4096,
                                             (1ull << 31));
-  uint64_t c = std::max<uint64_t>(1ull << 16, 4ull * (uint64_t)V + 2ull * (uint64_t)E / split);
+  uint64_t c = std::max<uint64_t>(1ull << 16, 8ull * (uint64_t)V + 2ull * (uint64_t)E / split);
   for (int i = 0; i < boost; i++) c *= 4;
   return (uint32_t)std::min(c, worst);
 }
@@ -396,8 +396,13 @@ struct Runner {
     c.DD = hop ? q->hop_bound + 1 : 1;
     c.RW = c.W * c.DD;
     c.hop = hop;
-    c.use_lb = hop ? 0 : 1;
-    c.use_tour = c.use_lb;
+    // The one-label and tour bounds of the unbounded problem are lower bounds of the
+    // hop-bounded one too (a hop-feasible completion is also an unbounded one), so
+    // hop-bounded queries prune with them against their own bound ub_cell.  Their
+    // distance search runs further (3 x the star bound), since ub_cell is larger.
+    c.use_lb = 1;
+    c.use_tour = 1;
+    c.cut_mult = hop ? 3u : 1u;
     for (int i = 0; i < q->k; i++) c.gid[i] = q->group_ids[i];
     memset(c.vv, 0xFF, sizeof(c.vv));
     c.delta = (uint32_t)std::max(0, eng->cfg.bucket_delta);
@@ -682,14 +687,17 @@ struct Runner {
     }
   }
 
-  // Summed profiled kernel time of this call (grow, rows, sssp), in ms.
-  void kernel_ms(double out[3]) {
+  // Summed profiled kernel time of this call (grow, rows, sssp), in ms, and launches.
+  void kernel_ms(double out[3], int64_t n[3]) {
     out[0] = out[1] = out[2] = 0;
+    n[0] = n[1] = n[2] = 0;
     for (auto& pr : cs.prof) {
       float e = 0;
       if (cudaEventElapsedTime(&e, eng->prof_events[2 * pr.second],
-                               eng->prof_events[2 * pr.second + 1]) == cudaSuccess)
+                               eng->prof_events[2 * pr.second + 1]) == cudaSuccess) {
         out[pr.first] += e;
+        n[pr.first]++;
+      }
     }
   }
 };
@@ -895,6 +903,13 @@ gst_status gst_engine_destroy(gst_engine* eng) {
   for (auto e : eng->prof_events) cudaEventDestroy(e);
   if (eng->pool) cudaMemPoolDestroy(eng->pool);
   delete eng;
+  return GST_OK;
+}
+
+gst_status gst_engine_set_profiling(gst_engine* eng, int32_t bits) {
+  if (!eng || bits < 0 || bits > 7) return fail(eng, GST_BAD_INPUT, "profiling: bits must be in [0, 7]");
+  std::lock_guard<std::mutex> lk(eng->mu);
+  eng->cfg.profile_kernels = bits;
   return GST_OK;
 }
 
@@ -1138,7 +1153,8 @@ gst_status gst_solve_batch(gst_graph* g, gst_groups* grp, int32_t n, const gst_q
             n, ms, (long long)R.cs.launches, (long long)R.cs.graph_launches,
             (long long)R.cs.graph_levels);
   double kms[3];
-  R.kernel_ms(kms);
+  int64_t kn[3];
+  R.kernel_ms(kms, kn);
   for (int32_t i = 0; i < n; i++) {
     gst_stats& s = results[i].stats;
     s.device_ms = ms;
@@ -1148,6 +1164,9 @@ gst_status gst_solve_batch(gst_graph* g, gst_groups* grp, int32_t n, const gst_q
     s.grow_ms = kms[PROF_GROW];
     s.rows_ms = kms[PROF_ROWS];
     s.sssp_ms = kms[PROF_SSSP];
+    s.grow_launches = kn[PROF_GROW];
+    s.rows_launches = kn[PROF_ROWS];
+    s.sssp_launches = kn[PROF_SSSP];
   }
   return GST_OK;
 }

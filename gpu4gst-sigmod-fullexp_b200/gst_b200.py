@@ -286,7 +286,8 @@ class Stats(C.Structure):
                 ("kernel_launches", C.c_int64), ("h2d_bytes", C.c_int64),
                 ("d2h_bytes", C.c_int64), ("device_ms", C.c_double), ("latency_ms", C.c_double),
                 ("grow_ms", C.c_double), ("rows_ms", C.c_double), ("sssp_ms", C.c_double),
-                ("queue_max", C.c_int64)]
+                ("queue_max", C.c_int64), ("grow_launches", C.c_int64),
+                ("rows_launches", C.c_int64), ("sssp_launches", C.c_int64)]
 
 
 class Result(C.Structure):
@@ -310,6 +311,7 @@ _sig("gst_groups_destroy", C.c_int, [_vp])
 _sig("gst_solve", C.c_int, [_vp, _vp, C.POINTER(Query), C.POINTER(Result)])
 _sig("gst_solve_batch", C.c_int, [_vp, _vp, C.c_int32, C.POINTER(Query), C.POINTER(Result)])
 _sig("gst_result_free", None, [C.POINTER(Result)])
+_sig("gst_engine_set_profiling", C.c_int, [_vp, C.c_int32])
 _sig("gst_server_create", C.c_int, [_vp, _vp, C.POINTER(_vp)])
 _sig("gst_submit", C.c_int, [_vp, C.POINTER(Query), C.POINTER(C.c_uint64)])
 _sig("gst_poll", C.c_int, [_vp, C.c_uint64, C.POINTER(Result)])
@@ -321,8 +323,16 @@ C_ABI_SYMBOLS = [
     "gst_graph_create", "gst_graph_create_i64", "gst_graph_destroy", "gst_groups_create",
     "gst_groups_destroy", "gst_solve", "gst_solve_batch", "gst_result_free",
     "gst_server_create", "gst_submit", "gst_poll", "gst_wait", "gst_server_destroy",
-    "gst_debug_slot_state", "gst_solve_noalloc",
+    "gst_debug_slot_state", "gst_solve_noalloc", "gst_engine_set_profiling",
 ]
+
+
+def set_profiling(eng: "Engine", bits: int) -> None:
+    """Bracket the grow (1) / rows (2) / sssp (4) launches of later solves with CUDA
+    events (include/gst.h: gst_engine_set_profiling)."""
+    rc = _lib.gst_engine_set_profiling(eng._h, bits)
+    if rc:
+        raise GstError(f"gst_engine_set_profiling: {STATUS.get(rc, rc)}")
 
 
 def default_config(**kw) -> Config:

@@ -94,6 +94,9 @@ typedef struct gst_stats {
   double rows_ms;           /*   (batch totals; 0 unless cfg.profile_kernels selects them) */
   double sssp_ms;
   int64_t queue_max;        /* largest worklist fill of the query (items) */
+  int64_t grow_launches;    /* profiled launches behind grow_ms / rows_ms / sssp_ms */
+  int64_t rows_launches;
+  int64_t sssp_launches;
 } gst_stats;
 
 typedef struct gst_result {
@@ -110,6 +113,10 @@ typedef struct gst_result {
 } gst_result;
 
 void gst_config_default(gst_config* cfg);
+/* Change cfg.profile_kernels of a live engine (bit0 grow, bit1 rows, bit2 sssp); the
+ * next solve brackets those launches with CUDA events (and runs the level loop
+ * without the CUDA graph while any bit is set). */
+gst_status gst_engine_set_profiling(gst_engine* eng, int32_t bits);
 
 gst_status gst_engine_create(int32_t device, const gst_config* cfg, gst_engine** out);
 gst_status gst_engine_destroy(gst_engine* eng);
