@@ -727,7 +727,7 @@ __host__ __device__ __forceinline__ size_t rows_smem_per_warp(int rw_max) {
 }
 
 // Dynamic shared memory per warp: RWmax cells + RWmax/32 pending words + RWmax list.
-__global__ void __launch_bounds__(256) k_rows(Ctx* ctxs, int nctx, DevGraph G, int split,
+__global__ void __launch_bounds__(256, 4) k_rows(Ctx* ctxs, int nctx, DevGraph G, int split,
                                               int rw_max) {
   __shared__ uint32_t s_pref[MAXB + 1];
   __shared__ uint32_t wcls[32];  // per warp: popcount classes holding pending cells
@@ -944,18 +944,56 @@ __global__ void __launch_bounds__(256) k_rows(Ctx* ctxs, int nctx, DevGraph G, i
       }
     }
     // emit the growing states, each relaxed from its lightest edge on (which lands
-    // at cst + 1 or later)
-    const uint32_t bend = c->bucket_end;
-    for (int i0 = 0; i0 < RW; i0 += 32) {
-      const int i = i0 + lane;
-      const bool want = i < RW && ((pend[i >> 5] >> (i & 31)) & 1u);
-      uint32_t gpd = 0, gcost = 0;
-      if (want) {
-        const uint32_t p = (uint32_t)i & full, d = (uint32_t)i >> k;
-        gpd = p | (d << 16);
-        gcost = cost_of(buf[i]);
+    // at cst + 1 or later): one reservation per list for the whole row
+    {
+      const uint32_t bend = c->bucket_end;
+      uint32_t cn = 0, cf = 0, kmin = COST_INF;
+      for (int i0 = 0; i0 < RW; i0 += 32) {
+        const int i = i0 + lane;
+        if (i < RW && ((pend[i >> 5] >> (i & 31)) & 1u)) {
+          const uint32_t key = cost_of(buf[i]) + 1u;
+          if (key >= bend) {
+            cf++;
+            kmin = min(kmin, key);
+          } else {
+            cn++;
+          }
+        }
       }
-      warp_append(ctxs, qi, want, (uint64_t)gcost + 1u >= bend, v, gpd, gcost, 0u, gcost + 1u);
+      const uint32_t sn = warp_incl_scan(cn), sf = warp_incl_scan(cf);
+      const uint32_t tn = __shfl_sync(0xffffffffu, sn, 31), tf = __shfl_sync(0xffffffffu, sf, 31);
+      kmin = __reduce_min_sync(0xffffffffu, kmin);
+      if (tn + tf > 0) {
+        uint32_t bn = 0, bfr = 0;
+        if (lane == 0) {
+          if (tn) bn = atomicAdd(&c->n_q[c->no], tn);
+          if (tf) {
+            bfr = atomicAdd(&c->n_far[c->f], tf);
+            atomicMin(&c->far_min, kmin);
+          }
+        }
+        bn = __shfl_sync(0xffffffffu, bn, 0) + sn - cn;
+        bfr = __shfl_sync(0xffffffffu, bfr, 0) + sf - cf;
+        uint4* nl = c->q[c->no];
+        uint4* fl = c->far[c->f];
+        for (int i0 = 0; i0 < RW; i0 += 32) {
+          const int i = i0 + lane;
+          if (i < RW && ((pend[i >> 5] >> (i & 31)) & 1u)) {
+            const uint32_t cst = cost_of(buf[i]);
+            const uint32_t p = (uint32_t)i & full, d = (uint32_t)i >> k;
+            const uint4 item = make_uint4(v, p | (d << 16), cst, 0u);
+            if (cst + 1u >= bend) {
+              if (bfr < c->farcap) fl[bfr] = item;
+              else atomicOr(&c->error, (uint32_t)ERR_FARCAP);
+              bfr++;
+            } else {
+              if (bn < c->qcap) nl[bn] = item;
+              else atomicOr(&c->error, (uint32_t)ERR_QCAP);
+              bn++;
+            }
+          }
+        }
+      }
     }
     // statistics: one atomic per query change of the warp, not per row
     if (qi != st_q) {

@@ -140,6 +140,8 @@ struct gst_graph {
   int2* d_edges = nullptr;   // per vertex sorted by neighbour (tree extraction)
   int2* d_wedges = nullptr;  // per vertex sorted by (weight, neighbour) (grow, SSSP)
   uint32_t* d_widx = nullptr;
+  int64_t max_deg = 0;       // shape of the graph (autotuner cache key)
+  int32_t max_w = 0;
   std::unique_ptr<Runner> batch;  // runner of gst_solve / gst_solve_batch (slots kept)
 };
 
@@ -209,6 +211,16 @@ int rows_blocks(gst_engine* eng, int threads, size_t smem) {
   const int blocks = eng->sms * std::min(per_sm, std::max(1, eng->cfg.blocks_per_sm));
   eng->rows_occ.push_back({key, blocks});
   return blocks;
+}
+
+// Launch geometry derived from the configuration (grids sized by occupancy).
+void apply_launch_config(gst_engine* eng) {
+  int occ_grow = 1, occ_sssp = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_grow, k_grow, 256, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sssp, k_sssp, 256, 0);
+  eng->grow_blocks = eng->sms * std::max(1, std::min(occ_grow, eng->cfg.blocks_per_sm));
+  eng->sssp_blocks = eng->sms * std::max(1, std::min(occ_sssp, eng->cfg.blocks_per_sm));
+  eng->rows_occ.clear();
 }
 
 enum ProfKind { PROF_GROW = 0, PROF_ROWS = 1, PROF_SSSP = 2 };
@@ -477,7 +489,7 @@ struct Runner {
       k_ctrl<<<nctx, 128, 0, st>>>(d_ctx, nctx, CTRL_SSSP);
     }
     const size_t per_warp = rows_smem_per_warp(rwm);
-    const int warps = std::max(1, tpb / 32);
+    const int warps = std::max(2, std::min(8, tpb / 32));  // k_rows: at most 256 threads
     int pe = prof ? prof_begin(PROF_ROWS) : -1;
     k_rows<<<rows_blocks(eng, warps * 32, per_warp * warps), warps * 32, per_warp * warps, st>>>(
         d_ctx, nctx, G, split, rwm);
@@ -513,7 +525,7 @@ struct Runner {
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     {
       // occupancy queries before the capture
-      const int warps = std::max(1, eng->cfg.threads_per_block / 32);
+      const int warps = std::max(2, std::min(8, eng->cfg.threads_per_block / 32));
       rows_blocks(eng, warps * 32, rows_smem_per_warp(rwm) * warps);
     }
     cudaStream_t cap;
@@ -861,7 +873,8 @@ gst_status gst_engine_create(int32_t device, const gst_config* cfg, gst_engine**
     if (eng->cfg.max_batch <= 0) eng->cfg.max_batch = d.max_batch;
     if (eng->cfg.use_graphs < 0) eng->cfg.use_graphs = 0;
   }
-  eng->cfg.threads_per_block = std::max(32, std::min(1024, eng->cfg.threads_per_block / 32 * 32));
+  // the rows kernel is compiled for at most 256 threads per CTA (4 CTAs per SM)
+  eng->cfg.threads_per_block = std::max(64, std::min(256, eng->cfg.threads_per_block / 32 * 32));
   eng->cfg.max_batch = std::min(eng->cfg.max_batch, MAXB);
   if (cudaSetDevice(device) != cudaSuccess) {
     delete eng;
@@ -870,11 +883,7 @@ gst_status gst_engine_create(int32_t device, const gst_config* cfg, gst_engine**
   cudaDeviceProp prop;
   cudaGetDeviceProperties(&prop, device);
   eng->sms = prop.multiProcessorCount;
-  int occ_grow = 1, occ_sssp = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_grow, k_grow, 256, 0);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sssp, k_sssp, 256, 0);
-  eng->grow_blocks = eng->sms * std::max(1, std::min(occ_grow, eng->cfg.blocks_per_sm));
-  eng->sssp_blocks = eng->sms * std::max(1, std::min(occ_sssp, eng->cfg.blocks_per_sm));
+  apply_launch_config(eng);
   // a pool of our own, keeping freed slot memory for the next query
   cudaMemPoolProps pp = {};
   pp.allocType = cudaMemAllocationTypePinned;
@@ -970,6 +979,8 @@ static gst_status graph_create_impl(gst_engine* eng, int64_t V, int64_t E, const
   g->eng = eng;
   g->V = V;
   g->E = E;
+  for (int64_t v = 0; v < V; v++) g->max_deg = std::max(g->max_deg, beg[v + 1] - beg[v]);
+  for (int64_t i = 0; i < E; i++) g->max_w = std::max(g->max_w, wt[i]);
   CK(cudaMalloc(&g->d_beg, sizeof(int64_t) * (V + 1)));
   CK(cudaMalloc(&g->d_edges, sizeof(int2) * std::max<int64_t>(E, 1)));
   CK(cudaMalloc(&g->d_wedges, sizeof(int2) * std::max<int64_t>(E, 1)));
@@ -1224,6 +1235,154 @@ void gst_result_free(gst_result* r) {
   free(r->edge_w);
   r->edge_u = r->edge_v = r->edge_w = nullptr;
   r->n_edges = 0;
+}
+
+// ---- autotuner ----------------------------------------------------------------------
+// Launch parameters are chosen per graph shape by coordinate descent on a sample of
+// queries: for each parameter in turn every candidate value is timed (device time
+// of gst_solve_batch on the sample, best of two) with the others held, and the
+// fastest is kept.  Every candidate must return the same costs; the result is
+// cached as one line per shape in a text file, so later runs on a graph of the same
+// shape skip the search.
+
+namespace {
+
+std::string shape_key(const gst_graph* g, int32_t max_batch) {
+  char b[160];
+  snprintf(b, sizeof b, "V=%lld E=%lld dmax=%lld wmax=%d batch=%d sms=%d", (long long)g->V,
+           (long long)g->E, (long long)g->max_deg, g->max_w, max_batch, g->eng->sms);
+  return b;
+}
+
+struct TuneParams {
+  int32_t split_degree, bucket_delta, threads_per_block, blocks_per_sm;
+};
+
+void set_params(gst_graph* g, const TuneParams& p) {
+  gst_engine* eng = g->eng;
+  eng->cfg.split_degree = p.split_degree;
+  eng->cfg.bucket_delta = p.bucket_delta;
+  eng->cfg.threads_per_block = std::max(64, std::min(256, p.threads_per_block / 32 * 32));
+  eng->cfg.blocks_per_sm = p.blocks_per_sm;
+  apply_launch_config(eng);
+  g->batch.reset();  // its CUDA graphs hold the old launch geometry
+}
+
+bool read_cache(const char* path, const std::string& key, TuneParams* p) {
+  if (!path) return false;
+  FILE* f = fopen(path, "r");
+  if (!f) return false;
+  char line[512];
+  bool hit = false;
+  while (fgets(line, sizeof line, f)) {
+    char* bar = strchr(line, '|');
+    if (!bar) continue;
+    *bar = 0;
+    if (key != line) continue;
+    TuneParams t;
+    if (sscanf(bar + 1, "%d %d %d %d", &t.split_degree, &t.bucket_delta, &t.threads_per_block,
+               &t.blocks_per_sm) == 4) {
+      *p = t;
+      hit = true;  // the last line for a key wins
+    }
+  }
+  fclose(f);
+  return hit;
+}
+
+}  // namespace
+
+extern "C" gst_status gst_autotune(gst_graph* g, gst_groups* grp, int32_t n,
+                                   const gst_query* sample, const char* cache_path,
+                                   gst_config* chosen) {
+  gst_engine* eng = g ? g->eng : nullptr;
+  if (!g || !grp || grp->g != g || n < 1 || !sample)
+    return fail(eng, GST_BAD_INPUT, "autotune: bad arguments");
+  const std::string key = shape_key(g, eng->cfg.max_batch);
+  TuneParams cur{eng->cfg.split_degree, eng->cfg.bucket_delta, eng->cfg.threads_per_block,
+                 eng->cfg.blocks_per_sm};
+  TuneParams hit;
+  if (read_cache(cache_path, key, &hit)) {
+    std::lock_guard<std::mutex> lk(eng->mu);
+    set_params(g, hit);
+    if (chosen) *chosen = eng->cfg;
+    return GST_OK;
+  }
+  const int32_t saved_prof = eng->cfg.profile_kernels;
+  eng->cfg.profile_kernels = 0;
+  std::vector<gst_result> res((size_t)n);
+  std::vector<int32_t> ref_cost((size_t)n), ref_status((size_t)n);
+  bool have_ref = false;
+  // device time of the sample under parameters p (best of two runs), or < 0 on failure
+  auto measure = [&](const TuneParams& p, double* ms) -> gst_status {
+    {
+      std::lock_guard<std::mutex> lk(eng->mu);
+      set_params(g, p);
+    }
+    double best = -1;
+    for (int rep = 0; rep < 2; rep++) {
+      gst_status st = gst_solve_batch(g, grp, n, sample, res.data());
+      if (st != GST_OK) return st;
+      const double t = res[0].stats.device_ms;
+      for (int32_t i = 0; i < n; i++) {
+        if (!have_ref) {
+          ref_cost[i] = res[i].cost;
+          ref_status[i] = res[i].status;
+        } else if (res[i].status != ref_status[i] ||
+                   (res[i].status == GST_OK && res[i].cost != ref_cost[i])) {
+          for (auto& r : res) gst_result_free(&r);
+          return fail(eng, GST_DEVICE_ERROR, "autotune: a candidate changed an optimum");
+        }
+        gst_result_free(&res[i]);
+      }
+      have_ref = true;
+      if (best < 0 || t < best) best = t;
+    }
+    *ms = best;
+    return GST_OK;
+  };
+  double best_ms = 0;
+  gst_status st = measure(cur, &best_ms);
+  const std::vector<int32_t> c_split = {64, 128, 256, 512, 1024};
+  const std::vector<int32_t> c_delta = {0, 2, 6, 16};
+  const std::vector<int32_t> c_tpb = {128, 256};
+  const std::vector<int32_t> c_bps = {2, 4, 8};
+  for (int param = 0; param < 4 && st == GST_OK; param++) {
+    const std::vector<int32_t>& cand =
+        param == 0 ? c_split : param == 1 ? c_delta : param == 2 ? c_tpb : c_bps;
+    for (int32_t v : cand) {
+      TuneParams p = cur;
+      int32_t* field = param == 0 ? &p.split_degree
+                       : param == 1 ? &p.bucket_delta
+                       : param == 2 ? &p.threads_per_block
+                                    : &p.blocks_per_sm;
+      if (*field == v) continue;
+      *field = v;
+      double ms = 0;
+      st = measure(p, &ms);
+      if (st != GST_OK) break;
+      if (ms < best_ms) {
+        best_ms = ms;
+        cur = p;
+      }
+    }
+  }
+  {
+    std::lock_guard<std::mutex> lk(eng->mu);
+    set_params(g, cur);
+    eng->cfg.profile_kernels = saved_prof;
+  }
+  if (st != GST_OK) return st;
+  if (cache_path) {
+    FILE* f = fopen(cache_path, "a");
+    if (f) {
+      fprintf(f, "%s|%d %d %d %d\n", key.c_str(), cur.split_degree, cur.bucket_delta,
+              cur.threads_per_block, cur.blocks_per_sm);
+      fclose(f);
+    }
+  }
+  if (chosen) *chosen = eng->cfg;
+  return GST_OK;
 }
 
 // ---- serving ---------------------------------------------------------------------

@@ -312,6 +312,8 @@ _sig("gst_solve", C.c_int, [_vp, _vp, C.POINTER(Query), C.POINTER(Result)])
 _sig("gst_solve_batch", C.c_int, [_vp, _vp, C.c_int32, C.POINTER(Query), C.POINTER(Result)])
 _sig("gst_result_free", None, [C.POINTER(Result)])
 _sig("gst_engine_set_profiling", C.c_int, [_vp, C.c_int32])
+_sig("gst_autotune", C.c_int, [_vp, _vp, C.c_int32, C.POINTER(Query), C.c_char_p,
+                               C.POINTER(Config)])
 _sig("gst_server_create", C.c_int, [_vp, _vp, C.POINTER(_vp)])
 _sig("gst_submit", C.c_int, [_vp, C.POINTER(Query), C.POINTER(C.c_uint64)])
 _sig("gst_poll", C.c_int, [_vp, C.c_uint64, C.POINTER(Result)])
@@ -323,7 +325,7 @@ C_ABI_SYMBOLS = [
     "gst_graph_create", "gst_graph_create_i64", "gst_graph_destroy", "gst_groups_create",
     "gst_groups_destroy", "gst_solve", "gst_solve_batch", "gst_result_free",
     "gst_server_create", "gst_submit", "gst_poll", "gst_wait", "gst_server_destroy",
-    "gst_debug_slot_state", "gst_solve_noalloc", "gst_engine_set_profiling",
+    "gst_debug_slot_state", "gst_solve_noalloc", "gst_engine_set_profiling", "gst_autotune",
 ]
 
 
@@ -465,6 +467,18 @@ class DeviceGraph:
 
     def server(self) -> "Server":
         return Server(self)
+
+    def autotune(self, group_ids_list, hop_bounds=None, cache_path: str | None = None) -> dict:
+        """Choose launch parameters for this graph's shape on a sample of queries
+        (include/gst.h: gst_autotune); returns the chosen settings."""
+        n = len(group_ids_list)
+        qs, keep = self._queries(group_ids_list, hop_bounds, None)
+        cfg = Config()
+        rc = _lib.gst_autotune(self._g, self._grp, n, qs,
+                               cache_path.encode() if cache_path else None, C.byref(cfg))
+        if rc:
+            raise GstError(f"gst_autotune: {STATUS.get(rc, rc)}: {self.eng.error()}")
+        return {f: getattr(cfg, f) for f, _ in Config._fields_}
 
 
 class Server:

@@ -60,7 +60,7 @@ typedef struct gst_config {
   int32_t split_degree;       /* edges per grow work item: hubs split into chunks of this size */
   int32_t bucket_delta;       /* cost-bucket width of the frontier ordering; 0 = autotune */
   int32_t max_levels;         /* per-query level budget (GST_TIMEOUT beyond) */
-  int32_t threads_per_block;  /* CTA size of the level kernels */
+  int32_t threads_per_block;  /* CTA size of the rows (merge) kernel, 64..256 */
   int32_t blocks_per_sm;      /* resident CTAs per SM for the level kernels */
   int32_t max_batch;          /* queries resident at once in gst_solve_batch / serving */
   int32_t use_graphs;         /* 1 (default): run the level loop as a CUDA graph whose
@@ -147,6 +147,19 @@ gst_status gst_solve_batch(gst_graph* g, gst_groups* grp, int32_t n, const gst_q
                            gst_result* results);
 
 void gst_result_free(gst_result* res);
+
+/* Autotuner (no counterpart in the reference, whose launch shapes are compile-time
+ * constants: BLKS_NUM / THDS_NUM in code/TrimCDP-WB/include/header.h and the 1024/512
+ * virtual-split degrees of graph.hpp:128-378).  Times the engine on the sample
+ * queries under candidate CTA sizes, hub-split (work chunk) sizes, cost-bucket
+ * widths and CTAs per SM, one parameter at a time, keeps the fastest setting in
+ * the engine, and appends it to the text file cache_path (NULL: no cache) under a
+ * key of the graph's shape (V, E, max degree, max weight, batch size, SM count).  A
+ * later call with a cached shape applies the cached setting without timing
+ * anything.  Every candidate must reproduce the sample's optimal costs, else
+ * GST_DEVICE_ERROR.  *chosen (may be NULL) receives the engine's new configuration. */
+gst_status gst_autotune(gst_graph* g, gst_groups* grp, int32_t n, const gst_query* sample,
+                        const char* cache_path, gst_config* chosen);
 
 /* Serving (no counterpart in the reference, whose drivers run a fixed query list;
  * this replaces the q_start..q_end loop of GSTnonHop.cu:247 / GPUHop.cu:172 for

@@ -1,0 +1,47 @@
+"""The autotuner picks launch parameters per graph shape, caches them, and never
+changes an optimum."""
+import os
+import time
+
+import pytest
+
+import gst_b200 as G
+from conftest import golden_inputs, load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+def test_autotune_caches_and_keeps_optima(tmp_path):
+    fx = load_golden("rmat3k_k4_k5")
+    g, grp = golden_inputs(fx)
+    case = fx["cases"][0]
+    qs = case["queries"][:8]
+    want = next(iter(case["ref"].values()))[:8]
+    cache = str(tmp_path / "tune.txt")
+    eng = G.Engine(0, max_batch=8)
+    dg = eng.graph(g, grp)
+    chosen = dg.autotune(qs, [case["hop"]] * len(qs), cache)
+    assert os.path.exists(cache)
+    with open(cache) as f:
+        lines = [l for l in f if l.strip()]
+    assert len(lines) == 1 and f"V={g.V} " in lines[0]
+    for key in ("split_degree", "bucket_delta", "threads_per_block", "blocks_per_sm"):
+        assert chosen[key] > 0 or key == "bucket_delta"
+    for q, c, a in zip(qs, want, dg.solve_batch(qs, [case["hop"]] * len(qs))):
+        assert a.ok and a.cost == c
+    dg.close()
+    eng.close()
+    # a fresh engine on the same shape takes the cached setting without timing
+    eng = G.Engine(0, max_batch=8)
+    dg = eng.graph(g, grp)
+    t0 = time.perf_counter()
+    again = dg.autotune(qs, [case["hop"]] * len(qs), cache)
+    assert time.perf_counter() - t0 < 1.0
+    assert all(again[k] == chosen[k] for k in ("split_degree", "bucket_delta",
+                                               "threads_per_block", "blocks_per_sm"))
+    with open(cache) as f:
+        assert len([l for l in f if l.strip()]) == 1
+    for q, c in zip(qs, want):
+        assert dg.solve(q, case["hop"]).cost == c
+    dg.close()
+    eng.close()
