@@ -719,10 +719,11 @@ __global__ void __launch_bounds__(256) k_grow(Ctx* ctxs, int nctx, DevGraph G, i
 }
 
 // ---- DP rows step: merge closure of dirty rows in shared memory -------------------
-// Per-warp shared memory: RW cells, RW/32 pending words, two lists of RW cell
-// indices (pending operands, finite partners), 16-B aligned.
+// Per-warp shared memory: RW cells, RW/32 pending words, RW/32 processed words, three
+// lists of RW cell indices (pending cells, finite cells, the cells of a round),
+// 16-B aligned.
 __host__ __device__ __forceinline__ size_t rows_smem_per_warp(int rw_max) {
-  const size_t b = (size_t)rw_max * 8 + (size_t)((rw_max + 31) / 32) * 4 + (size_t)rw_max * 4;
+  const size_t b = (size_t)rw_max * 8 + (size_t)((rw_max + 31) / 32) * 8 + (size_t)rw_max * 6;
   return (b + 15) & ~(size_t)15;
 }
 
@@ -730,7 +731,6 @@ __host__ __device__ __forceinline__ size_t rows_smem_per_warp(int rw_max) {
 __global__ void __launch_bounds__(256, 4) k_rows(Ctx* ctxs, int nctx, DevGraph G, int split,
                                               int rw_max) {
   __shared__ uint32_t s_pref[MAXB + 1];
-  __shared__ uint32_t wcls[32];  // per warp: popcount classes holding pending cells
   extern __shared__ __align__(16) unsigned char s_dyn[];
   load_prefix(ctxs, nctx, s_pref, -1);
   const uint32_t total = s_pref[nctx];
@@ -740,8 +740,11 @@ __global__ void __launch_bounds__(256, 4) k_rows(Ctx* ctxs, int nctx, DevGraph G
   unsigned char* wbase = s_dyn + per_warp * wib;
   unsigned long long* buf = (unsigned long long*)wbase;
   uint32_t* pend = (uint32_t*)(wbase + (size_t)rw_max * 8);
-  uint16_t* list = (uint16_t*)(wbase + (size_t)rw_max * 8 + (size_t)((rw_max + 31) / 32) * 4);
-  uint16_t* flist = list + rw_max;
+  uint32_t* done = pend + (rw_max + 31) / 32;
+  uint16_t* plist = (uint16_t*)(done + (rw_max + 31) / 32);
+  uint16_t* flist = plist + rw_max;
+  uint16_t* clist = flist + rw_max;
+  uint16_t* list = plist;  // reused for the tour-bound candidates after the closure
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int st_q = -1;
@@ -756,8 +759,8 @@ __global__ void __launch_bounds__(256, 4) k_rows(Ctx* ctxs, int nctx, DevGraph G
     (void)W;
     const uint32_t full = (uint32_t)c->full;
     unsigned long long* row = (unsigned long long*)&c->table[(uint64_t)v * RW];
-    // load row, collect pending bits and the popcount classes that hold pending cells
-    uint32_t cls = 0;
+    // load the row; list its pending cells (plist) and its finite cells (flist)
+    int np = 0, nf = 0;
     for (int i0 = 0; i0 < RW; i0 += 32) {
       const int i = i0 + lane;
       uint64_t x = CELL_INF;
@@ -766,81 +769,111 @@ __global__ void __launch_bounds__(256, 4) k_rows(Ctx* ctxs, int nctx, DevGraph G
         buf[i] = x;
       }
       // an unreached cell is all ones, so its pending bit must be ignored
-      const bool pn = i < RW && x != CELL_INF && ((uint32_t)x & PEND);
-      const uint32_t bal = __ballot_sync(0xffffffffu, pn);
-      if (pn) cls |= 1u << __popc((uint32_t)i & full);
-      if (lane == 0) pend[i0 >> 5] = bal;
+      const bool fin = i < RW && x != CELL_INF;
+      const bool pn = fin && ((uint32_t)x & PEND);
+      const bool fl = fin && ((uint32_t)i & full) != 0u;
+      const uint32_t bp = __ballot_sync(0xffffffffu, pn);
+      const uint32_t bf = __ballot_sync(0xffffffffu, fl);
+      const uint32_t lt = (1u << lane) - 1u;
+      if (pn) plist[np + __popc(bp & lt)] = (uint16_t)i;
+      if (fl) flist[nf + __popc(bf & lt)] = (uint16_t)i;
+      np += __popc(bp);
+      nf += __popc(bf);
+      if (lane == 0) {
+        pend[i0 >> 5] = bp;
+        done[i0 >> 5] = 0u;
+      }
     }
-    cls = __reduce_or_sync(0xffffffffu, cls);
-    if (lane == 0) {
-      wcls[wib] = cls;
-      atomicAnd(&c->rowbits[v >> 5], ~(1u << (v & 31)));
-    }
+    if (lane == 0) atomicAnd(&c->rowbits[v >> 5], ~(1u << (v & 31)));
     __syncwarp();
     const uint32_t ubm = hop ? c->ub_cell : c->ub;
-    // merge closure, by popcount class of the pending operand.  A pending cell X of
-    // class j is merged with every finite cell Y disjoint from it: either by
-    // enumerating the submasks of X's complement, or, when the row holds fewer
-    // finite partners than that, by scanning the list of finite cells.
-    for (int j = 1; j < k; j++) {
-      // classes without pending cells are skipped (merges that create or improve a
-      // cell of a higher class record it in wcls)
-      if (!((*(volatile uint32_t*)&wcls[wib] >> j) & 1u)) continue;
-      int nl = 0, nf = 0;
-      for (int i0 = 0; i0 < RW; i0 += 32) {
-        const int i = i0 + lane;
-        const uint32_t pc = i < RW ? (uint32_t)__popc((uint32_t)i & full) : 0u;
-        const bool sel = i < RW && ((pend[i >> 5] >> (i & 31)) & 1u) && pc == (uint32_t)j;
-        const bool fin = i < RW && pc >= 1u && pc <= (uint32_t)(k - j) &&
-                         cost_of(buf[i]) != COST_INF;
-        const uint32_t bal = __ballot_sync(0xffffffffu, sel);
-        const uint32_t bf = __ballot_sync(0xffffffffu, fin);
-        if (sel) list[nl + __popc(bal & ((1u << lane) - 1u))] = (uint16_t)i;
-        if (fin) flist[nf + __popc(bf & ((1u << lane) - 1u))] = (uint16_t)i;
-        nl += __popc(bal);
-        nf += __popc(bf);
+    // Merge closure T(v, X|Y) <= T(v, X) + T(v, Y), by rounds of popcount class: in a
+    // round the unprocessed pending cells X of the smallest class (clist) are merged
+    // with every finite cell Y disjoint from them, all pairs of the round spread
+    // over the lanes (partners from flist, or the submasks of ~X when flist is the
+    // longer).  Merges only create cells of a larger class, so a cell is final when
+    // its round comes; the cells a round creates or improves join plist (and flist).
+    for (;;) {
+      uint32_t mc = 0xFFFFFFFFu;
+      for (int t = lane; t < np; t += 32) {
+        const uint32_t cc = plist[t];
+        if (!((done[cc >> 5] >> (cc & 31)) & 1u)) mc = min(mc, (uint32_t)__popc(cc & full));
+      }
+      mc = __reduce_min_sync(0xffffffffu, mc);
+      if (mc >= (uint32_t)k) break;  // nothing left below the full set
+      int nl = 0;
+      for (int t0 = 0; t0 < np; t0 += 32) {
+        const int t = t0 + lane;
+        uint32_t cc = 0;
+        bool sel = false;
+        if (t < np) {
+          cc = plist[t];
+          sel = !((done[cc >> 5] >> (cc & 31)) & 1u) && (uint32_t)__popc(cc & full) == mc;
+        }
+        const uint32_t bs = __ballot_sync(0xffffffffu, sel);
+        if (sel) clist[nl + __popc(bs & ((1u << lane) - 1u))] = (uint16_t)cc;
+        nl += __popc(bs);
       }
       __syncwarp();
-      if (nl == 0 || nf == 0) continue;
-      const uint32_t m = (1u << (k - j)) - 1u;  // non-empty submasks of the complement
-      const bool scan_f = (uint32_t)nf < m * (uint32_t)DD;
+      for (int t = lane; t < nl; t += 32) {
+        const uint32_t cc = clist[t];
+        atomicOr(&done[cc >> 5], 1u << (cc & 31));
+      }
+      const uint32_t m = (1u << (k - (int)mc)) - 1u;  // non-empty submasks of ~X
+      const bool scan_f = (uint32_t)nf <= m * (uint32_t)DD;
       const uint32_t per = scan_f ? (uint32_t)nf : m * (uint32_t)DD;
       const uint32_t tp = (uint32_t)nl * per;
       merges += tp;
-      const float inv_per = 1.0f / (float)per;
+      const float inv_per = 1.0f / (float)max(per, 1u);
       const float inv_m = 1.0f / (float)m;
-      for (uint32_t t = lane; t < tp; t += 32) {
-        const uint32_t a = udiv_small(t, per, inv_per), r = t - a * per;
-        const uint32_t cell = list[a];
-        const uint32_t X = cell & full, d1 = cell >> k;
-        uint32_t Y, d2;
-        if (scan_f) {
-          const uint32_t yc = flist[r];
-          Y = yc & full;
-          d2 = yc >> k;
-          if (Y & X) continue;
-        } else {
-          // r = d2 * m + (yb - 1): partner hop d2, partner = yb-th submask of ~X
-          d2 = udiv_small(r, m, inv_m);
-          Y = deposit(r - d2 * m + 1u, full ^ X);
-        }
-        if (hop && (int)(d1 + d2) > D) continue;
-        if (!in_bounds(c, (d2 << k) + Y < (uint32_t)RW && (X | Y) < (uint32_t)W, 9)) continue;
-        const uint32_t cy = cost_of(buf[(d2 << k) + Y]);
-        if (cy == COST_INF) continue;
-        const uint32_t cand = cost_of(buf[cell]) + cy;
-        const uint32_t S = X | Y;
-        if (S != full && 3ull * cand > 2ull * ubm) continue;
-        const uint32_t nd = d1 > d2 ? d1 : d2;
-        const uint32_t tgt = (nd << k) + S;
-        const uint64_t nv = pack_cell(cand, PEND | MERGE | Y | (d2 << 16) | (d1 << 21));
-        if (nv < buf[tgt]) {
-          const uint64_t old = atomicMin(&buf[tgt], (unsigned long long)nv);
-          if (nv < old) {
-            atomicOr(&pend[tgt >> 5], 1u << (tgt & 31));
-            atomicOr(&wcls[wib], 1u << __popc(S));
+      __syncwarp();
+      for (uint32_t t0 = 0; t0 < tp; t0 += 32) {
+        const uint32_t t = t0 + lane;
+        bool newp = false, newf = false;
+        uint32_t tgt = 0;
+        if (t < tp) {
+          const uint32_t a = udiv_small(t, per, inv_per), r = t - a * per;
+          const uint32_t cell = clist[a];
+          const uint32_t X = cell & full, d1 = cell >> k;
+          uint32_t Y, d2;
+          if (scan_f) {
+            const uint32_t yc = flist[r];
+            Y = yc & full;
+            d2 = yc >> k;
+          } else {
+            // r = d2 * m + (yb - 1): partner hop d2, partner = yb-th submask of ~X
+            d2 = udiv_small(r, m, inv_m);
+            Y = deposit(r - d2 * m + 1u, full ^ X);
+          }
+          const uint32_t yi = (d2 << k) + Y;
+          const uint32_t cy = (Y & X) ? COST_INF : cost_of(buf[yi]);
+          const uint32_t S = X | Y;
+          const uint32_t cand = cost_of(buf[cell]) + cy;
+          bool ok = cy != COST_INF && !(hop && (int)(d1 + d2) > D) &&
+                    in_bounds(c, yi < (uint32_t)RW && S < (uint32_t)W, 9);
+          if (ok && S != full && 3ull * cand > 2ull * ubm) ok = false;
+          if (ok) {
+            const uint32_t nd = d1 > d2 ? d1 : d2;
+            tgt = (nd << k) + S;
+            const uint64_t nv = pack_cell(cand, PEND | MERGE | Y | (d2 << 16) | (d1 << 21));
+            if (nv < buf[tgt]) {
+              const uint64_t old = atomicMin(&buf[tgt], (unsigned long long)nv);
+              if (nv < old) {
+                newf = old == CELL_INF;
+                const uint32_t bit = 1u << (tgt & 31);
+                newp = !(atomicOr(&pend[tgt >> 5], bit) & bit);
+              }
+            }
           }
         }
+        // cells this step made pending or finite join the lists
+        const uint32_t bp = __ballot_sync(0xffffffffu, newp);
+        const uint32_t bf = __ballot_sync(0xffffffffu, newf);
+        const uint32_t lt = (1u << lane) - 1u;
+        if (newp) plist[np + __popc(bp & lt)] = (uint16_t)tgt;
+        if (newf) flist[nf + __popc(bf & lt)] = (uint16_t)tgt;
+        np += __popc(bp);
+        nf += __popc(bf);
       }
       __syncwarp();
     }
