@@ -309,6 +309,36 @@ def level_bytes(answers, queries, hops):
     return b
 
 
+def serve_run(dg, queries, hops, rate, n, seed):
+    """Poisson arrivals at `rate` queries/s through the continuous-batching server
+    (gst_submit / gst_wait); latency is the engine's time from submit to result."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / rate, n)
+    sv = dg.server()
+    tickets = []
+    t0 = time.perf_counter()
+    due = t0
+    for i in range(n):
+        due += gaps[i]
+        while True:
+            left = due - time.perf_counter()
+            if left <= 0:
+                break
+            if left > 2e-3:
+                time.sleep(left - 1e-3)
+        j = i % len(queries)
+        tickets.append(sv.submit(queries[j], hops[j], tag=i))
+    res = [sv.wait(t) for t in tickets]
+    t1 = time.perf_counter()
+    sv.close()
+    bad = [r for r in res if r.status not in (0, 1)]
+    lat = [r.stats["latency_ms"] for r in res]
+    return {"offered_qps": rate, "queries": n, "achieved_qps": n / (t1 - t0),
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "failed": len(bad)}
+
+
 def run_ours(args):
     import numpy as np
     import gst_b200 as G
@@ -386,6 +416,12 @@ def run_ours(args):
             per_q_host.append(time.perf_counter() - t0)
             per_q.append(a.stats["device_ms"])
 
+    # serving: Poisson arrivals at about 70 % of the batched throughput, ~3 s
+    serving = None
+    if rank == 0 and not args.no_serve:
+        rate = 0.7 * value / n_ranks
+        serving = serve_run(dg, queries, hops, rate, max(32, int(3.0 * rate)), SEED + 77)
+
     # roofline: the timed batches replayed with CUDA events around every level
     # kernel launch on the engine's stream (the timed region itself runs the
     # CUDA-graph loop, which has no per-kernel events)
@@ -435,6 +471,7 @@ def run_ours(args):
                       "queries": len(per_q),
                       "note": "same engine, gst_solve one query at a time"},
         "batched_over_per_query": (value / (len(per_q) / (sum(per_q) / 1e3))) if per_q else None,
+        "serving": serving,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": None, "kernel": top,
                      "peak_kind": peak_kind,
@@ -476,6 +513,7 @@ def main():
     ap.add_argument("--single", type=int, default=32, help="queries timed one at a time")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-tune", action="store_true", help="default launch parameters")
+    ap.add_argument("--no-serve", action="store_true", help="skip the Poisson serving run")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

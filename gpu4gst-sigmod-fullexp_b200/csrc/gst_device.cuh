@@ -618,7 +618,7 @@ __global__ void __launch_bounds__(256) k_sssp(Ctx* ctxs, int nctx, DevGraph G, i
 }
 
 // ---- DP grow step ----------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_grow(Ctx* ctxs, int nctx, DevGraph G, int split) {
+__global__ void __launch_bounds__(256, 3) k_grow(Ctx* ctxs, int nctx, DevGraph G, int split) {
   __shared__ uint32_t s_pref[MAXB + 1];
   load_prefix(ctxs, nctx, s_pref, PH_DP);
   const uint32_t total = s_pref[nctx];
@@ -697,6 +697,23 @@ __global__ void __launch_bounds__(256) k_grow(Ctx* ctxs, int nctx, DevGraph G, i
                                                                      ((uint64_t)d << c->k) + p])
                        : 0ull;
       }
+      // An improving target state (u, X) that cannot be part of a tree within the
+      // bound is not written at all: its cost plus the one-label bound
+      // max_{i not in X} d_i(u) already exceeds the bound (the same test the rows
+      // kernel applies before growing a state, here before it dirties a row).
+      uint4 da[RELAX_U], db[RELAX_U];
+#pragma unroll
+      for (int x = 0; x < RELAX_U; x++) {
+        Ctx* c = ctxs + x_qi[x];
+        const uint32_t u = (uint32_t)ed[x].x, nc = x_cost[x] + (uint32_t)ed[x].y;
+        ok[x] = ok[x] && pack_cell(nc, PEND | x_v[x]) < cur[x];
+        da[x] = db[x] = make_uint4(0, 0, 0, 0);
+        if (ok[x] && c->use_lb) {
+          const uint4* row = (const uint4*)&c->dist[(uint64_t)u * DIST_STRIDE];
+          da[x] = __ldcg(row);
+          db[x] = __ldcg(row + 1);
+        }
+      }
 #pragma unroll
       for (int x = 0; x < RELAX_U; x++) {
         Ctx* c = ctxs + x_qi[x];
@@ -704,11 +721,22 @@ __global__ void __launch_bounds__(256) k_grow(Ctx* ctxs, int nctx, DevGraph G, i
         bool dirty = false;
         if (ok[x]) {
           const uint32_t p = x_pd[x] & 0xFFFFu, d = (x_pd[x] >> 16) + (uint32_t)c->hop;
-          const uint64_t nv = pack_cell(nc, PEND | x_v[x]);
-          if (nv < cur[x]) {
+          if (c->use_lb) {
+            const uint32_t cut = c->cut;
+            const uint32_t lim = cut == COST_INF ? COST_INF : cut + 1u;
+            const uint32_t dd[8] = {da[x].x, da[x].y, da[x].z, da[x].w,
+                                    db[x].x, db[x].y, db[x].z, db[x].w};
+            const int k = c->k;
+            uint32_t lb = 0;
+#pragma unroll
+            for (int i = 0; i < KMAX; i++)
+              if (i < k && !((p >> i) & 1u)) lb = max(lb, min(dd[i], lim));
+            if ((uint64_t)nc + lb > (uint64_t)x_bound[x]) ok[x] = false;
+          }
+          if (ok[x]) {
             unsigned long long* tp =
                 (unsigned long long*)&c->table[(uint64_t)u * c->RW + ((uint64_t)d << c->k) + p];
-            const uint64_t old = atomicMin(tp, (unsigned long long)nv);
+            const uint64_t old = atomicMin(tp, (unsigned long long)pack_cell(nc, PEND | x_v[x]));
             dirty = cost_of(old) > nc;
           }
         }
