@@ -61,7 +61,7 @@ WORKLOADS = {
     "c4": dict(name="rmat4M_70M_k357_mixedD", graph=("rmat", 4_000_000, 70_000_000, SEED + 4),
                groups=("zipf", 20_000, 1.5, 2, 2000, SEED + 1004),
                queries=[(3, 410, SEED + 2041), (5, 410, SEED + 2042), (7, 204, SEED + 2043)],
-               hop=(4, 0.5, SEED + 3004)),
+               hop=(4, 0.5, SEED + 3004), tune_sample=16),
 }
 
 
@@ -368,9 +368,11 @@ def run_ours(args):
     tuned = None
     if not args.no_tune:
         cache = os.path.join(tempfile.gettempdir(), "gst_b200_autotune.txt")
-        tuned = dg.autotune(*batch(0), cache_path=cache)
+        tq, th = batch(0)
+        n_tune = w.get("tune_sample", len(tq))
+        tuned = dg.autotune(tq[:n_tune], th[:n_tune], cache_path=cache)
         tuned = {k: tuned[k] for k in ("split_degree", "bucket_delta", "threads_per_block",
-                                       "blocks_per_sm")}
+                                       "blocks_per_sm", "max_batch")}
     for s in range(args.warmup):
         dg.solve_batch(*batch(s))
 

@@ -241,6 +241,8 @@ struct Job {
 struct CallStats {
   int64_t launches = 0, h2d = 0, d2h = 0;
   int64_t graph_launches = 0, graph_levels = 0;
+  int64_t allocs = 0, alloc_bytes = 0;
+  double alloc_ms = 0;
   std::vector<std::pair<int, int>> prof;  // (kernel kind, event-pair index)
   size_t next_ev = 0;
 };
@@ -252,7 +254,17 @@ struct Runner {
   gst_groups* grp = nullptr;
   int max_slots;
   size_t budget = 0;            // bytes of slot memory the runner may hold
-  size_t held = 0;              // bytes of slot memory held now
+  size_t held = 0;              // bytes reserved from the pool (arenas)
+  // Slot memory is carved from a few large arenas taken from the pool (first fit,
+  // freed ranges coalesced): the pool maps physical memory for an allocation of a
+  // new size, which costs far more than a query at these sizes, so slots of
+  // varying size are sub-allocated from memory mapped once.
+  struct Arena {
+    unsigned char* base = nullptr;
+    size_t size = 0;
+    std::vector<std::pair<size_t, size_t>> free_;  // (offset, size), sorted by offset
+  };
+  std::vector<Arena> arenas;
   Ctx* d_ctx = nullptr;         // MAXB contexts
   Ctx* h_ctx = nullptr;         // pinned mirror
   uint32_t* d_loop = nullptr;   // graph loop: {iterations left, any query finished}
@@ -284,9 +296,9 @@ struct Runner {
       if (lg.graph) cudaGraphDestroy(lg.graph);
     }
     graphs.clear();
-    for (auto& m : mem)
-      if (m.base) cudaFreeAsync(m.base, eng->stream);
+    for (auto& a : arenas) cudaFreeAsync(a.base, eng->stream);
     cudaStreamSynchronize(eng->stream);
+    arenas.clear();
     mem.clear();
     held = 0;
     if (d_ctx) cudaFree(d_ctx);
@@ -329,18 +341,90 @@ struct Runner {
     return (int)r;
   }
 
-  // Free the memory of slots without a query, largest first, until `need` more
-  // bytes fit the budget.
-  void evict_idle(size_t need) {
-    while (held + need > budget) {
+  // First-fit range of `need` bytes from the arenas, or nullptr.
+  void* arena_take(size_t need) {
+    for (auto& a : arenas)
+      for (size_t i = 0; i < a.free_.size(); i++)
+        if (a.free_[i].second >= need) {
+          const size_t off = a.free_[i].first;
+          a.free_[i].first += need;
+          a.free_[i].second -= need;
+          if (a.free_[i].second == 0) a.free_.erase(a.free_.begin() + (long)i);
+          return a.base + off;
+        }
+    return nullptr;
+  }
+  // Return a range to its arena, merging it with free neighbours.
+  void arena_give(void* p, size_t n) {
+    for (auto& a : arenas) {
+      unsigned char* q = (unsigned char*)p;
+      if (q < a.base || q >= a.base + a.size) continue;
+      const size_t off = (size_t)(q - a.base);
+      auto it = std::lower_bound(a.free_.begin(), a.free_.end(), std::make_pair(off, (size_t)0));
+      it = a.free_.insert(it, {off, n});
+      const size_t i = (size_t)(it - a.free_.begin());
+      if (i + 1 < a.free_.size() && a.free_[i].first + a.free_[i].second == a.free_[i + 1].first) {
+        a.free_[i].second += a.free_[i + 1].second;
+        a.free_.erase(a.free_.begin() + (long)i + 1);
+      }
+      if (i > 0 && a.free_[i - 1].first + a.free_[i - 1].second == a.free_[i].first) {
+        a.free_[i - 1].second += a.free_[i].second;
+        a.free_.erase(a.free_.begin() + (long)i);
+      }
+      return;
+    }
+  }
+  // Reserve a new arena of at least `need` bytes (4 GB chunks) within the budget.
+  gst_status arena_grow(size_t need, bool* grown) {
+    *grown = false;
+    if (held + need > budget) return GST_OK;
+    const size_t chunk = std::max(need, std::min((size_t)4 << 30, budget - held));
+    void* p = nullptr;
+    const auto ta = Clock::now();
+    CK(cudaMallocFromPoolAsync(&p, chunk, eng->pool, eng->stream));
+    cs.alloc_ms += std::chrono::duration<double, std::milli>(Clock::now() - ta).count();
+    cs.allocs++;
+    cs.alloc_bytes += (int64_t)chunk;
+    Arena a;
+    a.base = (unsigned char*)p;
+    a.size = chunk;
+    a.free_.push_back({0, chunk});
+    arenas.push_back(a);
+    held += chunk;
+    *grown = true;
+    return GST_OK;
+  }
+  // Memory of `need` bytes for a slot: a free range, else after returning idle
+  // slots' memory (largest first), else from a new arena; nullptr if none fits.
+  gst_status slot_memory(size_t need, void** out) {
+    *out = arena_take(need);
+    while (!*out) {
       int best = -1;
       for (int s = 0; s < (int)mem.size(); s++)
         if (!owner[s] && mem[s].base && (best < 0 || mem[s].bytes > mem[best].bytes)) best = s;
-      if (best < 0) return;
-      cudaFreeAsync(mem[best].base, eng->stream);
-      held -= mem[best].bytes;
+      if (best < 0) break;
+      arena_give(mem[best].base, mem[best].bytes);
       mem[best] = SlotMem();
+      *out = arena_take(need);
     }
+    if (!*out) {
+      // hand wholly free arenas back to the pool while a new one would not fit
+      for (size_t i = 0; i < arenas.size() && held + need > budget;) {
+        Arena& a = arenas[i];
+        if (a.free_.size() == 1 && a.free_[0].first == 0 && a.free_[0].second == a.size) {
+          cudaFreeAsync(a.base, eng->stream);
+          held -= a.size;
+          arenas.erase(arenas.begin() + (long)i);
+        } else {
+          i++;
+        }
+      }
+      bool grown = false;
+      gst_status st = arena_grow(need, &grown);
+      if (st != GST_OK) return st;
+      if (grown) *out = arena_take(need);
+    }
+    return GST_OK;
   }
 
   // Put job j into a free slot.  GST_OK: admitted.  GST_NOT_READY: no slot or
@@ -364,20 +448,18 @@ struct Runner {
         if (!owner[i]) s = i;
       if (s < 0) return GST_NOT_READY;
       if (mem[s].base) {
-        cudaFreeAsync(mem[s].base, eng->stream);
-        held -= mem[s].bytes;
+        arena_give(mem[s].base, mem[s].bytes);
         mem[s] = SlotMem();
       }
-      evict_idle(need);
-      if (held + need > budget) return GST_NOT_READY;
       void* p = nullptr;
-      CK(cudaMallocFromPoolAsync(&p, need, eng->pool, eng->stream));
+      gst_status st = slot_memory(need, &p);
+      if (st != GST_OK) return st;
+      if (!p) return GST_NOT_READY;
       SlotMem m;
       carve_slot(m, (unsigned char*)p, g->V, j->rw, cap, farcap);
       m.base = p;
       m.bytes = need;
       mem[s] = m;
-      held += need;
     }
     SlotMem& m = mem[s];
     // fresh context
@@ -1160,9 +1242,10 @@ gst_status gst_solve_batch(gst_graph* g, gst_groups* grp, int32_t n, const gst_q
     return fail(eng, st, msg);
   }
   if (eng->cfg.verbose)
-    fprintf(stderr, "[gst batch] %d queries: %.3f ms, %lld launches, %lld graph launches, %lld graph levels\n",
+    fprintf(stderr, "[gst batch] %d queries: %.3f ms, %lld launches, %lld graph launches, %lld graph levels, "
+            "%lld slot allocations (%.1f GB, %.1f ms host)\n",
             n, ms, (long long)R.cs.launches, (long long)R.cs.graph_launches,
-            (long long)R.cs.graph_levels);
+            (long long)R.cs.graph_levels, (long long)R.cs.allocs, R.cs.alloc_bytes / 1e9, R.cs.alloc_ms);
   double kms[3];
   int64_t kn[3];
   R.kernel_ms(kms, kn);
@@ -1255,7 +1338,7 @@ std::string shape_key(const gst_graph* g, int32_t max_batch) {
 }
 
 struct TuneParams {
-  int32_t split_degree, bucket_delta, threads_per_block, blocks_per_sm;
+  int32_t split_degree, bucket_delta, threads_per_block, blocks_per_sm, max_batch;
 };
 
 void set_params(gst_graph* g, const TuneParams& p) {
@@ -1264,6 +1347,7 @@ void set_params(gst_graph* g, const TuneParams& p) {
   eng->cfg.bucket_delta = p.bucket_delta;
   eng->cfg.threads_per_block = std::max(64, std::min(256, p.threads_per_block / 32 * 32));
   eng->cfg.blocks_per_sm = p.blocks_per_sm;
+  eng->cfg.max_batch = std::max(1, std::min(MAXB, p.max_batch));
   apply_launch_config(eng);
   g->batch.reset();  // its CUDA graphs hold the old launch geometry
 }
@@ -1280,8 +1364,8 @@ bool read_cache(const char* path, const std::string& key, TuneParams* p) {
     *bar = 0;
     if (key != line) continue;
     TuneParams t;
-    if (sscanf(bar + 1, "%d %d %d %d", &t.split_degree, &t.bucket_delta, &t.threads_per_block,
-               &t.blocks_per_sm) == 4) {
+    if (sscanf(bar + 1, "%d %d %d %d %d", &t.split_degree, &t.bucket_delta, &t.threads_per_block,
+               &t.blocks_per_sm, &t.max_batch) == 5) {
       *p = t;
       hit = true;  // the last line for a key wins
     }
@@ -1300,7 +1384,7 @@ extern "C" gst_status gst_autotune(gst_graph* g, gst_groups* grp, int32_t n,
     return fail(eng, GST_BAD_INPUT, "autotune: bad arguments");
   const std::string key = shape_key(g, eng->cfg.max_batch);
   TuneParams cur{eng->cfg.split_degree, eng->cfg.bucket_delta, eng->cfg.threads_per_block,
-                 eng->cfg.blocks_per_sm};
+                 eng->cfg.blocks_per_sm, eng->cfg.max_batch};
   TuneParams hit;
   if (read_cache(cache_path, key, &hit)) {
     std::lock_guard<std::mutex> lk(eng->mu);
@@ -1347,15 +1431,22 @@ extern "C" gst_status gst_autotune(gst_graph* g, gst_groups* grp, int32_t n,
   const std::vector<int32_t> c_delta = {0, 2, 6, 16};
   const std::vector<int32_t> c_tpb = {128, 256};
   const std::vector<int32_t> c_bps = {2, 4, 8};
-  for (int param = 0; param < 4 && st == GST_OK; param++) {
-    const std::vector<int32_t>& cand =
-        param == 0 ? c_split : param == 1 ? c_delta : param == 2 ? c_tpb : c_bps;
+  std::vector<int32_t> c_batch;  // resident queries: at most the configured batch
+  for (int32_t b : {4, 8, 16, 32, 64})
+    if (b < cur.max_batch) c_batch.push_back(b);
+  for (int param = 0; param < 5 && st == GST_OK; param++) {
+    const std::vector<int32_t>& cand = param == 0   ? c_split
+                                       : param == 1 ? c_delta
+                                       : param == 2 ? c_tpb
+                                       : param == 3 ? c_bps
+                                                    : c_batch;
     for (int32_t v : cand) {
       TuneParams p = cur;
-      int32_t* field = param == 0 ? &p.split_degree
+      int32_t* field = param == 0   ? &p.split_degree
                        : param == 1 ? &p.bucket_delta
                        : param == 2 ? &p.threads_per_block
-                                    : &p.blocks_per_sm;
+                       : param == 3 ? &p.blocks_per_sm
+                                    : &p.max_batch;
       if (*field == v) continue;
       *field = v;
       double ms = 0;
@@ -1376,8 +1467,8 @@ extern "C" gst_status gst_autotune(gst_graph* g, gst_groups* grp, int32_t n,
   if (cache_path) {
     FILE* f = fopen(cache_path, "a");
     if (f) {
-      fprintf(f, "%s|%d %d %d %d\n", key.c_str(), cur.split_degree, cur.bucket_delta,
-              cur.threads_per_block, cur.blocks_per_sm);
+      fprintf(f, "%s|%d %d %d %d %d\n", key.c_str(), cur.split_degree, cur.bucket_delta,
+              cur.threads_per_block, cur.blocks_per_sm, cur.max_batch);
       fclose(f);
     }
   }

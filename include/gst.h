@@ -152,7 +152,8 @@ void gst_result_free(gst_result* res);
  * constants: BLKS_NUM / THDS_NUM in code/TrimCDP-WB/include/header.h and the 1024/512
  * virtual-split degrees of graph.hpp:128-378).  Times the engine on the sample
  * queries under candidate CTA sizes, hub-split (work chunk) sizes, cost-bucket
- * widths and CTAs per SM, one parameter at a time, keeps the fastest setting in
+ * widths, CTAs per SM and numbers of resident queries (at most cfg.max_batch), one
+ * parameter at a time, keeps the fastest setting in
  * the engine, and appends it to the text file cache_path (NULL: no cache) under a
  * key of the graph's shape (V, E, max degree, max weight, batch size, SM count).  A
  * later call with a cached shape applies the cached setting without timing

@@ -25,7 +25,8 @@ def test_autotune_caches_and_keeps_optima(tmp_path):
     with open(cache) as f:
         lines = [l for l in f if l.strip()]
     assert len(lines) == 1 and f"V={g.V} " in lines[0]
-    for key in ("split_degree", "bucket_delta", "threads_per_block", "blocks_per_sm"):
+    for key in ("split_degree", "bucket_delta", "threads_per_block", "blocks_per_sm",
+                "max_batch"):
         assert chosen[key] > 0 or key == "bucket_delta"
     for q, c, a in zip(qs, want, dg.solve_batch(qs, [case["hop"]] * len(qs))):
         assert a.ok and a.cost == c
@@ -38,7 +39,8 @@ def test_autotune_caches_and_keeps_optima(tmp_path):
     again = dg.autotune(qs, [case["hop"]] * len(qs), cache)
     assert time.perf_counter() - t0 < 1.0
     assert all(again[k] == chosen[k] for k in ("split_degree", "bucket_delta",
-                                               "threads_per_block", "blocks_per_sm"))
+                                               "threads_per_block", "blocks_per_sm",
+                                               "max_batch"))
     with open(cache) as f:
         assert len([l for l in f if l.strip()]) == 1
     for q, c in zip(qs, want):
