@@ -1432,7 +1432,7 @@ extern "C" gst_status gst_autotune(gst_graph* g, gst_groups* grp, int32_t n,
   const std::vector<int32_t> c_tpb = {128, 256};
   const std::vector<int32_t> c_bps = {2, 4, 8};
   std::vector<int32_t> c_batch;  // resident queries: at most the configured batch
-  for (int32_t b : {4, 8, 16, 32, 64})
+  for (int32_t b : {1, 2, 4, 8, 16, 32, 64})
     if (b < cur.max_batch) c_batch.push_back(b);
   for (int param = 0; param < 5 && st == GST_OK; param++) {
     const std::vector<int32_t>& cand = param == 0   ? c_split
