@@ -355,7 +355,7 @@ def run_ours(args):
     w, g, grp, queries, hops = make_workload(args.workload)
     B = args.batch
     # the product path: CUDA-graph level loop, no per-kernel events
-    eng = G.Engine(local_rank, max_batch=min(B, 64))
+    eng = G.Engine(local_rank, max_batch=min(B, 64), use_graphs=0 if args.no_graphs else 1)
     dg = eng.graph(g, grp)
 
     # each rank takes its own slice of the query stream (replicas, weak scaling)
@@ -523,6 +523,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-tune", action="store_true", help="default launch parameters")
     ap.add_argument("--no-serve", action="store_true", help="skip the Poisson serving run")
+    ap.add_argument("--no-graphs", action="store_true",
+                    help="host-issued level launches instead of the CUDA-graph loop "
+                         "(profilers then see every kernel launch)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -496,7 +496,7 @@ struct Runner {
     // distance search runs further (3 x the star bound), since ub_cell is larger.
     c.use_lb = 1;
     c.use_tour = 1;
-    c.cut_mult = hop ? 3u : 1u;
+    c.cut_mult = hop ? (uint32_t)(eng->cfg.hop_cut_mult > 0 ? eng->cfg.hop_cut_mult : 3) : 1u;
     for (int i = 0; i < q->k; i++) c.gid[i] = q->group_ids[i];
     memset(c.vv, 0xFF, sizeof(c.vv));
     c.delta = (uint32_t)std::max(0, eng->cfg.bucket_delta);
@@ -932,6 +932,7 @@ void gst_config_default(gst_config* cfg) {
   cfg->max_batch = 16;
   cfg->use_graphs = 1;
   cfg->verbose = 0;
+  cfg->hop_cut_mult = 3;
 }
 
 gst_status gst_engine_create(int32_t device, const gst_config* cfg, gst_engine** out) {
@@ -954,6 +955,7 @@ gst_status gst_engine_create(int32_t device, const gst_config* cfg, gst_engine**
     if (eng->cfg.blocks_per_sm <= 0) eng->cfg.blocks_per_sm = d.blocks_per_sm;
     if (eng->cfg.max_batch <= 0) eng->cfg.max_batch = d.max_batch;
     if (eng->cfg.use_graphs < 0) eng->cfg.use_graphs = 0;
+    if (eng->cfg.hop_cut_mult <= 0) eng->cfg.hop_cut_mult = 3;
   }
   // the rows kernel is compiled for at most 256 threads per CTA (4 CTAs per SM)
   eng->cfg.threads_per_block = std::max(64, std::min(256, eng->cfg.threads_per_block / 32 * 32));

@@ -69,6 +69,9 @@ typedef struct gst_config {
   int32_t profile_kernels;    /* bit0 grow, bit1 rows, bit2 sssp: bracket those launches with
                                  CUDA events and report their summed device time */
   int32_t verbose;
+  int32_t hop_cut_mult;       /* hop-bounded queries: the distance search stops at this
+                                 multiple of the star bound (0 = 3); larger prunes more
+                                 DP states and costs a longer search */
 } gst_config;
 
 typedef struct gst_query {
