@@ -309,6 +309,25 @@ def level_bytes(answers, queries, hops):
     return b
 
 
+def rank_slice(n_queries, step, B, rank, n_ranks):
+    """Query indices of `rank`'s batch at `step`: every rank takes its own slice of
+    the query stream (replicas, weak scaling), the ranks' slices of a step disjoint
+    while B * n_ranks <= n_queries."""
+    base = ((step * n_ranks + rank) * B) % n_queries
+    return [(base + i) % n_queries for i in range(B)]
+
+
+def max_over_ranks(values, dist):
+    """Element-wise max over the ranks of a list of floats (gloo all-reduce; the
+    identity for one process)."""
+    if dist is None:
+        return list(values)
+    import torch
+    t = torch.tensor(values, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
 def serve_run(dg, queries, hops, rate, n, seed):
     """Poisson arrivals at `rate` queries/s through the continuous-batching server
     (gst_submit / gst_wait); latency is the engine's time from submit to result."""
@@ -358,10 +377,8 @@ def run_ours(args):
     eng = G.Engine(local_rank, max_batch=min(B, 64), use_graphs=0 if args.no_graphs else 1)
     dg = eng.graph(g, grp)
 
-    # each rank takes its own slice of the query stream (replicas, weak scaling)
     def batch(step):
-        base = ((step * n_ranks + rank) * B) % len(queries)
-        idx = [(base + i) % len(queries) for i in range(B)]
+        idx = rank_slice(len(queries), step, B, rank, n_ranks)
         return [queries[i] for i in idx], [hops[i] for i in idx]
 
     # launch parameters for this graph shape, chosen on the first batch (cached)
@@ -399,12 +416,7 @@ def run_ours(args):
             d2h += st["d2h_bytes"]
             launches += st["kernel_launches"]
     torch.cuda.synchronize()
-    tot_dev = sum(dev_ms) / 1e3
-    tot_host = sum(host_ms) / 1e3
-    if dist:
-        t = torch.tensor([tot_dev, tot_host], dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot_dev, tot_host = float(t[0]), float(t[1])
+    tot_dev, tot_host = max_over_ranks([sum(dev_ms) / 1e3, sum(host_ms) / 1e3], dist)
     nq_all = args.steps * B * n_ranks
     value = nq_all / tot_dev
     e2e = nq_all / tot_host
