@@ -64,6 +64,9 @@ enum CtrlMode : int { CTRL_SSSP = 0, CTRL_DP_ROWS = 1, CTRL_DP_GROW = 2 };
 constexpr int WIDX = 16;
 constexpr uint32_t CHUNK = 0x80000000u;  // item flag (in pd): one `split`-edge chunk only
 constexpr int RELAX_U = 4;               // edges per lane per round of the relax loops
+// Hop-limited distance items carry their path's edge count in bits 8..15 of the
+// group word (group index in bits 0..7).
+constexpr uint32_t SSSP_HOP_SHIFT = 8;
 constexpr int TOUR_STRIDE = KMAX * KMAX;
 
 struct DevGraph {
@@ -136,6 +139,8 @@ struct Ctx {
                         // above it (or unreached) is only known to exceed it
   uint32_t cut_mult;    // the distance search stops at cut_mult x ub (hop-bounded queries
                         // prune against their own, larger, bound and want more of them)
+  uint32_t sssp_hops;   // 0: distances d_i(v); D: hop-limited distances d_i^{<=D}(v), the
+                        // cheapest paths of at most D edges (hop-bounded queries)
   uint32_t ub_cell;     // best full-state cell
   unsigned long long best;  // cost<<32 | d<<27 | v of the best full-state cell
   uint32_t phase;
@@ -328,12 +333,13 @@ struct Plan {
   uint32_t off, key;
   uint32_t spawn;   // chunk items to append at offsets off + n + j * split
 };
-__device__ __forceinline__ Plan plan_item(const DevGraph& G, uint32_t v, uint32_t cost, uint32_t off,
-                                          uint32_t wmax, uint32_t bucket_end, int split,
-                                          bool chunk) {
+// b0, b1: v's row offsets, loaded by the caller together with the item's other
+// loads (they depend only on v), so that planning adds one dependent load, the
+// light-edge count.
+__device__ __forceinline__ Plan plan_item(const DevGraph& G, uint32_t v, int64_t b0, int64_t b1,
+                                          uint32_t cost, uint32_t off, uint32_t wmax,
+                                          uint32_t bucket_end, int split, bool chunk) {
   Plan P{0, 0u, false, false, 0u, 0u, 0u};
-  // the loads below depend only on the item, so they are issued together
-  const int64_t b0 = G.beg[v], b1 = G.beg[v + 1];
   const int64_t deg = b1 - b0;
   const uint64_t in_bucket = bucket_end > cost ? (uint64_t)bucket_end - cost - 1u : 0u;
   const uint32_t hw = (uint32_t)min((uint64_t)wmax, in_bucket);
@@ -468,10 +474,18 @@ __global__ void k_init(Ctx* ctxs, int nctx, DevGraph G, const int64_t* grp_ptr,
         mark_row(c, v);
         if (c->phase == PH_SSSP) {
           const uint32_t old = atomicMin(&c->dist[(uint64_t)v * DIST_STRIDE + i], 0u);
-          if (old != 0u && G.beg[v + 1] > G.beg[v]) {
-            const uint32_t n = atomicAdd(&c->n_q[c->no], 1u);
-            if (n < c->qcap) c->q[c->no][n] = make_uint4(v, (uint32_t)i, 0u, 0u);
-            else atomicOr(&c->error, (uint32_t)ERR_QCAP);
+          const int64_t deg = G.beg[v + 1] - G.beg[v];
+          if (old != 0u && deg > 0) {
+            // unlimited distances: one head item; hop-limited: every chunk at once,
+            // so that all edges of a round are relaxed in the same step
+            const uint32_t nch =
+                c->sssp_hops ? (uint32_t)((deg + split - 1) / split) : 1u;
+            const uint32_t pd = c->sssp_hops ? ((uint32_t)i | CHUNK) : (uint32_t)i;
+            const uint32_t n = atomicAdd(&c->n_q[c->no], nch);
+            for (uint32_t j = 0; j < nch; j++) {
+              if (n + j < c->qcap) c->q[c->no][n + j] = make_uint4(v, pd, 0u, j * (uint32_t)split);
+              else atomicOr(&c->error, (uint32_t)ERR_QCAP);
+            }
           }
         }
       }
@@ -503,15 +517,20 @@ __global__ void __launch_bounds__(256) k_sssp(Ctx* ctxs, int nctx, DevGraph G, i
       gi = e.y;
       cost = e.z;
       e_off = e.w;
-      if (in_bounds(c, v < G.V && (gi & ~CHUNK) < (uint32_t)c->k, 2)) {
-        const uint32_t cur = __ldcg(&c->dist[(uint64_t)v * DIST_STRIDE + (gi & ~CHUNK)]);
+      const uint32_t g = gi & 0xFFu;
+      if (in_bounds(c, v < G.V && g < (uint32_t)c->k, 2)) {
+        const int64_t b0 = G.beg[v], b1 = G.beg[v + 1];
+        const uint32_t cur = __ldcg(&c->dist[(uint64_t)v * DIST_STRIDE + g]);
         // ub is read once per item (a per-edge read of one word by every thread of
         // a one-query launch is an L2 hot spot); a stale, larger ub prunes less
         ub = sssp_cutoff(c);
         bend = c->bucket_end;
-        // not stale, and still able to reach a vertex at distance <= ub
-        if (cur >= cost && cost < ub)
-          P = plan_item(G, v, cost, e.w, ub - cost, bend, split, (gi & CHUNK) != 0u);
+        // not stale, and still able to reach a vertex at distance <= ub.  A hop-
+        // limited item is relaxed even when its vertex has a cheaper distance
+        // since: that distance may use more edges, and the item's own path of
+        // fewer edges can still reach further within the hop limit.
+        if ((cur >= cost || c->sssp_hops) && cost < ub)
+          P = plan_item(G, v, b0, b1, cost, e.w, ub - cost, bend, split, (gi & CHUNK) != 0u);
       }
       gi &= ~CHUNK;
     }
@@ -551,15 +570,18 @@ __global__ void __launch_bounds__(256) k_sssp(Ctx* ctxs, int nctx, DevGraph G, i
         // distances above ub are never needed exactly: a state whose missing group
         // lies further than ub is pruned whatever the exact distance
         ok[x] = ok[x] && in_bounds(ctxs + x_qi[x], u < G.V, 4) && nd <= x_ub[x];
-        cur[x] = ok[x] ? __ldcg(&ctxs[x_qi[x]].dist[(uint64_t)u * DIST_STRIDE + x_gi[x]]) : 0u;
+        cur[x] = ok[x] ? __ldcg(&ctxs[x_qi[x]].dist[(uint64_t)u * DIST_STRIDE + (x_gi[x] & 0xFFu)])
+                       : 0u;
       }
 #pragma unroll
       for (int x = 0; x < RELAX_U; x++) {
         const uint32_t u = (uint32_t)ed[x].x, nd = x_cost[x] + (uint32_t)ed[x].y;
         Ctx* c = ctxs + x_qi[x];
+        const uint32_t grp = x_gi[x] & 0xFFu, hops = x_gi[x] >> SSSP_HOP_SHIFT;
         bool push = false;
+        uint32_t nch = 0;
         if (ok[x] && nd < cur[x]) {
-          const uint32_t old = atomicMin(&c->dist[(uint64_t)u * DIST_STRIDE + x_gi[x]], nd);
+          const uint32_t old = atomicMin(&c->dist[(uint64_t)u * DIST_STRIDE + grp], nd);
           if (nd < old) {
             // star bound from tentative distances: the k paths found so far from u
             // to a member of each group form a connected subgraph covering every
@@ -571,15 +593,25 @@ __global__ void __launch_bounds__(256) k_sssp(Ctx* ctxs, int nctx, DevGraph G, i
             uint64_t sum = 0;
 #pragma unroll
             for (int i = 0; i < KMAX; i++)
-              if (i < k) sum += (i == (int)x_gi[x]) ? nd : d[i];
+              if (i < k) sum += (i == (int)grp) ? nd : d[i];
             if (sum < (uint64_t)x_ub[x]) atomicMin(&c->ub, (uint32_t)sum);
-            push = nd < x_ub[x];
+            if (!c->sssp_hops) {
+              push = nd < x_ub[x];
+            } else if (hops + 1u < c->sssp_hops && nd < x_ub[x]) {
+              // hop-limited: the next round relaxes u's edges, all of its chunks in
+              // the same step (one round = one edge more)
+              const int64_t ub0 = G.beg[u], ub1 = G.beg[u + 1];
+              const int64_t cnt = count_upto(G, u, ub1 - ub0, x_ub[x] - nd);
+              nch = (uint32_t)((cnt + split - 1) / split);
+            }
           }
         }
         // an improved vertex relaxes its own edges from the lightest one, which lands
         // at nd + 1 or later: in this bucket or a later one
         const bool far = (uint64_t)nd + 1u >= x_bend[x];
-        warp_append(ctxs, x_qi[x], push, far, u, x_gi[x], nd, 0u, nd + 1u);
+        warp_append(ctxs, x_qi[x], push, far, u, grp, nd, 0u, nd + 1u);
+        warp_append_chunks(ctxs, x_qi[x], nch, u, grp | ((hops + 1u) << SSSP_HOP_SHIFT), nd, 0u,
+                           split);
       }
     }
   }
@@ -642,6 +674,7 @@ __global__ void __launch_bounds__(256, 3) k_grow(Ctx* ctxs, int nctx, DevGraph G
       e_off = e.w;
       const uint32_t p = pd & 0xFFFFu, d = pd >> 16;
       const bool ok = in_bounds(c, v < G.V && p < (uint32_t)c->W && d < (uint32_t)c->DD, 5);
+      const int64_t b0 = ok ? G.beg[v] : 0, b1 = ok ? G.beg[v + 1] : 0;
       const uint64_t cell = ok ? __ldcg((const unsigned long long*)&c->table[(uint64_t)v * c->RW +
                                                                            ((uint64_t)d << c->k) + p])
                                : 0ull;
@@ -651,7 +684,7 @@ __global__ void __launch_bounds__(256, 3) k_grow(Ctx* ctxs, int nctx, DevGraph G
       if (ok && src_ok && cost_of(cell) >= cost && 2ull * cost <= (uint64_t)bound) {
         const uint32_t wmax = c->hop ? (bound > cost ? bound - cost - 1u : 0u)
                                      : (bound >= cost ? bound - cost : 0u);
-        P = plan_item(G, v, cost, e.w, wmax, c->bucket_end, split, chunk);
+        P = plan_item(G, v, b0, b1, cost, e.w, wmax, c->bucket_end, split, chunk);
       }
     }
     warp_append(ctxs, qi, P.push, P.far, v, pd, cost, P.off, P.key);

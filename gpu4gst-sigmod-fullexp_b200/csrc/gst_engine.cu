@@ -492,18 +492,22 @@ struct Runner {
     c.hop = hop;
     // The one-label and tour bounds of the unbounded problem are lower bounds of the
     // hop-bounded one too (a hop-feasible completion is also an unbounded one), so
-    // hop-bounded queries prune with them against their own bound ub_cell.  Their
-    // distance search runs further (3 x the star bound), since ub_cell is larger.
+    // hop-bounded queries prune with them against their own bound ub_cell.
     c.use_lb = 1;
     c.use_tour = 1;
-    c.cut_mult = hop ? (uint32_t)(eng->cfg.hop_cut_mult > 0 ? eng->cfg.hop_cut_mult : 3) : 1u;
+    c.cut_mult = hop ? (uint32_t)(eng->cfg.hop_cut_mult > 0 ? eng->cfg.hop_cut_mult : 1) : 1u;
+    // A tree of diameter <= D reaches every missing group within D edges of any of its
+    // vertices, so hop-bounded queries bound with the cheapest paths of at most D
+    // edges (a level-synchronous search of D rounds), tighter than unlimited ones.
+    c.sssp_hops = hop && q->hop_bound > 0 ? (uint32_t)q->hop_bound : 0u;
     for (int i = 0; i < q->k; i++) c.gid[i] = q->group_ids[i];
     memset(c.vv, 0xFF, sizeof(c.vv));
     c.delta = (uint32_t)std::max(0, eng->cfg.bucket_delta);
     c.max_levels = (uint32_t)eng->cfg.max_levels;
     c.in_idx = 1;
     c.far_min = 0xFFFFFFFFu;
-    c.bucket_end = c.delta ? c.delta : 0xFFFFFFFFu;
+    // the hop-limited search runs one round per step, in one cost bucket
+    c.bucket_end = c.delta && !c.sssp_hops ? c.delta : 0xFFFFFFFFu;
     c.ub = 0xFFFFFFFFu;
     c.cut = 0xFFFFFFFFu;
     c.ub_cell = 0xFFFFFFFFu;
@@ -932,7 +936,7 @@ void gst_config_default(gst_config* cfg) {
   cfg->max_batch = 16;
   cfg->use_graphs = 1;
   cfg->verbose = 0;
-  cfg->hop_cut_mult = 3;
+  cfg->hop_cut_mult = 1;
 }
 
 gst_status gst_engine_create(int32_t device, const gst_config* cfg, gst_engine** out) {
@@ -955,7 +959,7 @@ gst_status gst_engine_create(int32_t device, const gst_config* cfg, gst_engine**
     if (eng->cfg.blocks_per_sm <= 0) eng->cfg.blocks_per_sm = d.blocks_per_sm;
     if (eng->cfg.max_batch <= 0) eng->cfg.max_batch = d.max_batch;
     if (eng->cfg.use_graphs < 0) eng->cfg.use_graphs = 0;
-    if (eng->cfg.hop_cut_mult <= 0) eng->cfg.hop_cut_mult = 3;
+    if (eng->cfg.hop_cut_mult <= 0) eng->cfg.hop_cut_mult = 1;
   }
   // the rows kernel is compiled for at most 256 threads per CTA (4 CTAs per SM)
   eng->cfg.threads_per_block = std::max(64, std::min(256, eng->cfg.threads_per_block / 32 * 32));

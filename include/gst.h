@@ -70,7 +70,7 @@ typedef struct gst_config {
                                  CUDA events and report their summed device time */
   int32_t verbose;
   int32_t hop_cut_mult;       /* hop-bounded queries: the distance search stops at this
-                                 multiple of the star bound (0 = 3); larger prunes more
+                                 multiple of the star bound (0 = 1); larger prunes more
                                  DP states and costs a longer search */
 } gst_config;
 
