@@ -69,6 +69,13 @@ SPECS = [
      "groups": {"kind": "zipf", "n": 1000, "s": 1.5, "smin": 2, "smax": 200, "seed": 92},
      "queries": [{"k": 6, "n": 20, "seed": 93, "hop": [None, 3]}],
      "solvers": ["PrunedDP++", "D-PrunedDP++"]},
+    # hop-bounded queries at a larger scale (the hop-limited lower bounds prune hard)
+    {"name": "rmat50k_hop",
+     "graph": {"kind": "rmat", "V": 50000, "E": 400000, "seed": 101},
+     "groups": {"kind": "zipf", "n": 2000, "s": 1.5, "smin": 2, "smax": 300, "seed": 102},
+     "queries": [{"k": 4, "n": 16, "seed": 103, "hop": [2, 4, 5]},
+                 {"k": 5, "n": 12, "seed": 104, "hop": [None, 3, 4]}],
+     "solvers": ["PrunedDP++", "D-PrunedDP++"]},
 ]
 
 
@@ -122,14 +129,16 @@ KNOWN_ANSWER = {
 }
 
 
-def main():
-    fixtures = [run_spec(s) for s in SPECS]
+def main(names=None):
+    """Regenerate every fixture, or only the named ones."""
+    fixtures = [run_spec(s) for s in SPECS if not names or s["name"] in names]
     for f in fixtures:
         with open(os.path.join(HERE, f["name"] + ".json"), "w") as fh:
             json.dump(f, fh, separators=(",", ":"))
-    with open(os.path.join(HERE, "known_answer.json"), "w") as fh:
-        json.dump(KNOWN_ANSWER, fh, indent=1)
+    if not names:
+        with open(os.path.join(HERE, "known_answer.json"), "w") as fh:
+            json.dump(KNOWN_ANSWER, fh, indent=1)
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -16,11 +16,12 @@ def _ref_cost(c):
     return -1 if c >= REF_INF else c
 
 
-@pytest.mark.parametrize("name", ["c1_ba20k_k3", "rmat3k_k4_k5", "rmat20k_k6"])
+@pytest.mark.parametrize("name", ["c1_ba20k_k3", "rmat3k_k4_k5", "rmat20k_k6", "rmat50k_hop"])
 def test_oracle_matches_reference_golden(name):
     fx = load_golden(name)
     g, grp = golden_inputs(fx)
-    limit = 10 if name == "rmat20k_k6" else None  # the k=6 DP takes seconds per query here
+    # the larger DPs take about a second per query here
+    limit = {"rmat20k_k6": 10, "rmat50k_hop": 4}.get(name)
     for case in fx["cases"]:
         qs = case["queries"][:limit]
         for solver, costs in case["ref"].items():
