@@ -765,6 +765,25 @@ __global__ void __launch_bounds__(256, 3) k_grow(Ctx* ctxs, int nctx, DevGraph G
             for (int i = 0; i < KMAX; i++)
               if (i < k && !((p >> i) & 1u)) lb = max(lb, min(dd[i], lim));
             if ((uint64_t)nc + lb > (uint64_t)x_bound[x]) ok[x] = false;
+            if (ok[x] && c->use_tour && p != (uint32_t)c->full) {
+              // the O(k) half of the tour bound (see the rows kernel): twice the rest
+              // of any tree holding (u, p) costs at least
+              // max_a d_a(u) + min_b P(a,b,Xb) + min_b d_b(u) over groups a, b not in p
+              const uint32_t Xb = (uint32_t)c->full ^ p;
+              const uint32_t* W2 = c->tour + (size_t)c->W * TOUR_STRIDE + (size_t)Xb * KMAX;
+              uint32_t mind = COST_INF;
+#pragma unroll
+              for (int i = 0; i < KMAX; i++)
+                if (i < k && ((Xb >> i) & 1u)) mind = min(mind, min(dd[i], lim));
+              uint64_t lb2 = 0;
+#pragma unroll
+              for (int i = 0; i < KMAX; i++)
+                if (i < k && ((Xb >> i) & 1u)) {
+                  const uint64_t t2 = (uint64_t)min(dd[i], lim) + __ldg(&W2[i]) + mind;
+                  lb2 = t2 > lb2 ? t2 : lb2;
+                }
+              if ((uint64_t)nc + (lb2 + 1) / 2 > (uint64_t)x_bound[x]) ok[x] = false;
+            }
           }
           if (ok[x]) {
             unsigned long long* tp =
