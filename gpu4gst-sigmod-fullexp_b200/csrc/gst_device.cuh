@@ -109,6 +109,9 @@ struct Ctx {
   uint64_t* table;
   uint32_t* dist;
   uint32_t* rowbits;
+  uint32_t* fm[2];     // group-mask frontier (one byte per vertex, four to a word): the
+                       // groups whose distance at the vertex improved in the step that
+                       // wrote fm[no]; read and cleared by the next step through fm[in_idx]
   uint32_t* tour;      // 2^k x TOUR_STRIDE path table, then 2^k x KMAX row minima
   uint4* q[2];
   uint4* far[2];
@@ -141,6 +144,8 @@ struct Ctx {
                         // prune against their own, larger, bound and want more of them)
   uint32_t sssp_hops;   // 0: distances d_i(v); D: hop-limited distances d_i^{<=D}(v), the
                         // cheapest paths of at most D edges (hop-bounded queries)
+  uint32_t sssp_mask;   // 1: the distance search runs one item per (vertex, group mask)
+                        // (unlimited distances in one cost bucket); 0: one per (vertex, group)
   uint32_t ub_cell;     // best full-state cell
   unsigned long long best;  // cost<<32 | d<<27 | v of the best full-state cell
   uint32_t phase;
@@ -475,7 +480,16 @@ __global__ void k_init(Ctx* ctxs, int nctx, DevGraph G, const int64_t* grp_ptr,
         if (c->phase == PH_SSSP) {
           const uint32_t old = atomicMin(&c->dist[(uint64_t)v * DIST_STRIDE + i], 0u);
           const int64_t deg = G.beg[v + 1] - G.beg[v];
-          if (old != 0u && deg > 0) {
+          if (old != 0u && deg > 0 && c->sssp_mask) {
+            // group-mask items: one head item per vertex, the groups in fm
+            const uint32_t sh = (v & 3u) * 8u;
+            const uint32_t ow = atomicOr(&c->fm[c->no][v >> 2], (1u << i) << sh);
+            if (((ow >> sh) & 0xFFu) == 0u) {
+              const uint32_t n = atomicAdd(&c->n_q[c->no], 1u);
+              if (n < c->qcap) c->q[c->no][n] = make_uint4(v, 0u, 0u, 0u);
+              else atomicOr(&c->error, (uint32_t)ERR_QCAP);
+            }
+          } else if (old != 0u && deg > 0) {
             // unlimited distances: one head item; hop-limited: every chunk at once,
             // so that all edges of a round are relaxed in the same step
             const uint32_t nch =
@@ -494,14 +508,30 @@ __global__ void k_init(Ctx* ctxs, int nctx, DevGraph G, const int64_t* grp_ptr,
 }
 
 // ---- one-label SSSP step: multi-source Bellman-Ford with near/far ordering ----
-// Work item {v, group index i, dist, chunk}: relax dist_i(u) for u in the chunk.
-// (code/TrimCDP-WB/include/mapper_enactor.cuh:249-366 computes the same
-// distances as grow-only DP states (v, 1<<i).)
-__global__ void __launch_bounds__(256) k_sssp(Ctx* ctxs, int nctx, DevGraph G, int split) {
+// Two item forms (code/TrimCDP-WB/include/mapper_enactor.cuh:249-366 computes the
+// same distances as grow-only DP states (v, 1<<i)):
+//  - group items {v, group index i [| hops << 8], dist, offset}: relax d_i(u) for the
+//    edges of the item (hop-limited searches, and searches in cost buckets);
+//  - group-mask items (sssp_mask, unlimited distances in one bucket): a head item
+//    {v, 0, 0, 0} takes the groups whose d_i(v) improved in the previous step from
+//    fm[in_idx] (and clears them); a chunk item {v, mask | CHUNK, 0, offset} carries
+//    its groups.  Each edge is read once for all of the item's groups and the
+//    target's 32-byte distance row once, and a vertex improved for several groups in
+//    one step is queued once.  Items relax with the distances current when they run
+//    (a value at most the one announced), and a distance written in a step is
+//    announced in fm of that step, read only by the next launch, so every write is
+//    visible to the item that its bit schedules.
+constexpr uint32_t SSSP_MASKED = 0x40000000u;  // lane-local flag: a group-mask item
+constexpr int SSSP_U = 2;                      // edges per lane per round of the relax loop
+__global__ void __launch_bounds__(256, 4) k_sssp(Ctx* ctxs, int nctx, DevGraph G, int split) {
   __shared__ uint32_t s_pref[MAXB + 1];
+  // per warp and lane: the distances of the lane's group-mask item (COST_INF for
+  // groups outside its mask), read by the lanes that relax its edges
+  __shared__ uint4 s_dv[256 / 32][32][2];
   load_prefix(ctxs, nctx, s_pref, PH_SSSP);
   const uint32_t total = s_pref[nctx];
   const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   for (uint32_t base = wid * 32; base < total; base += warps * 32) {
@@ -509,6 +539,9 @@ __global__ void __launch_bounds__(256) k_sssp(Ctx* ctxs, int nctx, DevGraph G, i
     uint32_t v = 0, gi = 0, cost = 0, ub = 0, bend = 0, e_off = 0;
     int qi = 0;
     Plan P{0, 0u, false, false, 0u, 0u, 0u};
+    uint32_t dv[KMAX];
+#pragma unroll
+    for (int i = 0; i < KMAX; i++) dv[i] = COST_INF;
     if (it < total) {
       qi = find_ctx(s_pref, nctx, it);
       Ctx* c = ctxs + qi;
@@ -518,7 +551,36 @@ __global__ void __launch_bounds__(256) k_sssp(Ctx* ctxs, int nctx, DevGraph G, i
       cost = e.z;
       e_off = e.w;
       const uint32_t g = gi & 0xFFu;
-      if (in_bounds(c, v < G.V && g < (uint32_t)c->k, 2)) {
+      if (c->sssp_mask) {
+        if (in_bounds(c, v < G.V, 2)) {
+          const int64_t b0 = G.beg[v], b1 = G.beg[v + 1];
+          uint32_t m;
+          if (gi & CHUNK) {
+            m = g;
+          } else {
+            unsigned char* fb = (unsigned char*)c->fm[c->in_idx] + v;
+            m = __ldcg(fb);
+            *fb = 0;
+          }
+          const uint4* row = (const uint4*)&c->dist[(uint64_t)v * DIST_STRIDE];
+          const uint4 a = __ldcg(row), b = __ldcg(row + 1);
+          const uint32_t d[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+          ub = sssp_cutoff(c);
+          bend = COST_INF;
+          const int k = c->k;
+          uint32_t mind = COST_INF, mk = 0;
+#pragma unroll
+          for (int i = 0; i < KMAX; i++)
+            if (i < k && ((m >> i) & 1u) && d[i] < ub) {
+              dv[i] = d[i];
+              mind = min(mind, d[i]);
+              mk |= 1u << i;
+            }
+          cost = mind;
+          gi = mk | SSSP_MASKED | ((uint32_t)k << 24);
+          if (mk) P = plan_item(G, v, b0, b1, mind, e.w, ub - mind, bend, split, (e.y & CHUNK) != 0u);
+        }
+      } else if (in_bounds(c, v < G.V && g < (uint32_t)c->k, 2)) {
         const int64_t b0 = G.beg[v], b1 = G.beg[v + 1];
         const uint32_t cur = __ldcg(&c->dist[(uint64_t)v * DIST_STRIDE + g]);
         // ub is read once per item (a per-edge read of one word by every thread of
@@ -534,53 +596,104 @@ __global__ void __launch_bounds__(256) k_sssp(Ctx* ctxs, int nctx, DevGraph G, i
       }
       gi &= ~CHUNK;
     }
+    s_dv[wib][lane][0] = make_uint4(dv[0], dv[1], dv[2], dv[3]);
+    s_dv[wib][lane][1] = make_uint4(dv[4], dv[5], dv[6], dv[7]);
+    __syncwarp();
     warp_append(ctxs, qi, P.push, P.far, v, gi, cost, P.off, P.key);
-    warp_append_chunks(ctxs, qi, P.spawn, v, gi, cost, e_off + P.n, split);
+    warp_append_chunks(ctxs, qi, P.spawn, v, (gi & SSSP_MASKED) ? (gi & 0xFFu) : gi, cost,
+                       e_off + P.n, split);
     const uint32_t n = P.n;
     const int64_t eb = P.eb;
     add_stat(ctxs, qi, it < total, n, &Ctx::st_sssp);
     const uint32_t scan = warp_incl_scan(n);
     const uint32_t tot = __shfl_sync(0xffffffffu, scan, 31);
-    // RELAX_U edges per lane per round: their loads are independent, so a warp has
-    // RELAX_U edge loads, then RELAX_U distance loads, in flight at once
-    for (uint32_t j0 = 0; j0 < tot; j0 += 32 * RELAX_U) {
-      int2 ed[RELAX_U];
-      uint32_t x_gi[RELAX_U], x_cost[RELAX_U], x_ub[RELAX_U], x_bend[RELAX_U], cur[RELAX_U];
-      int x_qi[RELAX_U];
-      bool ok[RELAX_U];
+    // SSSP_U edges per lane per round: their loads are independent, so a warp has
+    // SSSP_U edge loads, then SSSP_U distance loads, in flight at once
+    for (uint32_t j0 = 0; j0 < tot; j0 += 32 * SSSP_U) {
+      int2 ed[SSSP_U];
+      uint32_t x_gi[SSSP_U], x_cost[SSSP_U], x_ub[SSSP_U], x_o[SSSP_U];
+      uint4 ra[SSSP_U], rb[SSSP_U];  // target's distance row (ra.x alone for group items)
+      int x_qi[SSSP_U];
+      bool ok[SSSP_U];
 #pragma unroll
-      for (int x = 0; x < RELAX_U; x++) {
+      for (int x = 0; x < SSSP_U; x++) {
         const uint32_t j = j0 + (uint32_t)x * 32u + lane;
         const int o = warp_owner(scan, j < tot ? j : tot - 1);
         const uint32_t o_scan = __shfl_sync(0xffffffffu, scan, o);
         const uint32_t o_n = __shfl_sync(0xffffffffu, n, o);
         const int64_t o_eb = __shfl_sync(0xffffffffu, eb, o);
+        x_o[x] = (uint32_t)o;
         x_gi[x] = __shfl_sync(0xffffffffu, gi, o);
         x_cost[x] = __shfl_sync(0xffffffffu, cost, o);
         x_ub[x] = __shfl_sync(0xffffffffu, ub, o);
-        x_bend[x] = __shfl_sync(0xffffffffu, bend, o);
         x_qi[x] = __shfl_sync(0xffffffffu, qi, o);
         const uint32_t off = j - (o_scan - o_n);
         ok[x] = j < tot && in_bounds(ctxs + x_qi[x], o_eb + off < G.E, 3);
         ed[x] = ok[x] ? G.wedges[o_eb + off] : make_int2(0, 0);
       }
 #pragma unroll
-      for (int x = 0; x < RELAX_U; x++) {
+      for (int x = 0; x < SSSP_U; x++) {
         const uint32_t u = (uint32_t)ed[x].x, nd = x_cost[x] + (uint32_t)ed[x].y;
         // distances above ub are never needed exactly: a state whose missing group
-        // lies further than ub is pruned whatever the exact distance
+        // lies further than ub is pruned whatever the exact distance (for a group-mask
+        // item, cost is its smallest distance)
         ok[x] = ok[x] && in_bounds(ctxs + x_qi[x], u < G.V, 4) && nd <= x_ub[x];
-        cur[x] = ok[x] ? __ldcg(&ctxs[x_qi[x]].dist[(uint64_t)u * DIST_STRIDE + (x_gi[x] & 0xFFu)])
-                       : 0u;
+        const uint32_t* drow = ctxs[x_qi[x]].dist + (uint64_t)u * DIST_STRIDE;
+        ra[x] = make_uint4(0u, 0u, 0u, 0u);
+        rb[x] = make_uint4(COST_INF, COST_INF, COST_INF, COST_INF);
+        if (ok[x] && (x_gi[x] & SSSP_MASKED)) {
+          ra[x] = __ldcg((const uint4*)drow);
+          if (((x_gi[x] >> 24) & 0xFu) > 4u) rb[x] = __ldcg((const uint4*)drow + 1);
+        } else if (ok[x]) {
+          ra[x].x = __ldcg(drow + (x_gi[x] & 0xFFu));
+        }
       }
 #pragma unroll
-      for (int x = 0; x < RELAX_U; x++) {
-        const uint32_t u = (uint32_t)ed[x].x, nd = x_cost[x] + (uint32_t)ed[x].y;
+      for (int x = 0; x < SSSP_U; x++) {
+        const uint32_t u = (uint32_t)ed[x].x, w = (uint32_t)ed[x].y, nd = x_cost[x] + w;
         Ctx* c = ctxs + x_qi[x];
-        const uint32_t grp = x_gi[x] & 0xFFu, hops = x_gi[x] >> SSSP_HOP_SHIFT;
-        bool push = false;
-        uint32_t nch = 0;
-        if (ok[x] && nd < cur[x]) {
+        bool push = false, far = false;
+        uint32_t nch = 0, p_gi = 0, p_cost = 0, c_gi = 0;
+        if (ok[x] && (x_gi[x] & SSSP_MASKED)) {
+          // group-mask edge: every group of the owner's item whose distance through
+          // this edge beats the target's
+          const uint4 oa = s_dv[wib][x_o[x]][0], ob = s_dv[wib][x_o[x]][1];
+          const uint32_t od[8] = {oa.x, oa.y, oa.z, oa.w, ob.x, ob.y, ob.z, ob.w};
+          uint32_t cu[8] = {ra[x].x, ra[x].y, ra[x].z, ra[x].w, rb[x].x, rb[x].y, rb[x].z, rb[x].w};
+          const int k = (int)((x_gi[x] >> 24) & 0xFu);
+          const uint32_t lim = x_ub[x];
+          uint32_t imp = 0, ext = 0;
+#pragma unroll
+          for (int i = 0; i < KMAX; i++) {
+            if (i < k && od[i] < lim && w <= lim - od[i]) {
+              const uint32_t ndi = od[i] + w;
+              if (ndi < cu[i]) {
+                const uint32_t old = atomicMin(&c->dist[(uint64_t)u * DIST_STRIDE + i], ndi);
+                if (ndi < old) {
+                  imp |= 1u << i;
+                  if (ndi < lim) ext |= 1u << i;
+                }
+                cu[i] = min(ndi, old);
+              }
+            }
+          }
+          if (imp) {
+            // star bound (see below): the k shortest paths found so far from u
+            uint64_t sum = 0;
+#pragma unroll
+            for (int i = 0; i < KMAX; i++)
+              if (i < k) sum += cu[i];
+            if (sum < (uint64_t)lim) atomicMin(&c->ub, (uint32_t)sum);
+          }
+          if (ext) {
+            // announce the improved groups to the next step; the first announcement
+            // of u in this step queues it
+            const uint32_t sh = (u & 3u) * 8u;
+            const uint32_t ow = atomicOr(&c->fm[c->no][u >> 2], ext << sh);
+            push = ((ow >> sh) & 0xFFu) == 0u;
+          }
+        } else if (ok[x] && nd < ra[x].x) {
+          const uint32_t grp = x_gi[x] & 0xFFu, hops = x_gi[x] >> SSSP_HOP_SHIFT;
           const uint32_t old = atomicMin(&c->dist[(uint64_t)u * DIST_STRIDE + grp], nd);
           if (nd < old) {
             // star bound from tentative distances: the k paths found so far from u
@@ -597,23 +710,27 @@ __global__ void __launch_bounds__(256) k_sssp(Ctx* ctxs, int nctx, DevGraph G, i
             if (sum < (uint64_t)x_ub[x]) atomicMin(&c->ub, (uint32_t)sum);
             if (!c->sssp_hops) {
               push = nd < x_ub[x];
+              // an improved vertex relaxes its own edges from the lightest one, which
+              // lands at nd + 1 or later: in this bucket or a later one
+              far = (uint64_t)nd + 1u >= c->bucket_end;
+              p_gi = grp;
+              p_cost = nd;
             } else if (hops + 1u < c->sssp_hops && nd < x_ub[x]) {
               // hop-limited: the next round relaxes u's edges, all of its chunks in
               // the same step (one round = one edge more)
               const int64_t ub0 = G.beg[u], ub1 = G.beg[u + 1];
               const int64_t cnt = count_upto(G, u, ub1 - ub0, x_ub[x] - nd);
               nch = (uint32_t)((cnt + split - 1) / split);
+              c_gi = grp | ((hops + 1u) << SSSP_HOP_SHIFT);
+              p_cost = nd;
             }
           }
         }
-        // an improved vertex relaxes its own edges from the lightest one, which lands
-        // at nd + 1 or later: in this bucket or a later one
-        const bool far = (uint64_t)nd + 1u >= x_bend[x];
-        warp_append(ctxs, x_qi[x], push, far, u, grp, nd, 0u, nd + 1u);
-        warp_append_chunks(ctxs, x_qi[x], nch, u, grp | ((hops + 1u) << SSSP_HOP_SHIFT), nd, 0u,
-                           split);
+        warp_append(ctxs, x_qi[x], push, far, u, p_gi, p_cost, 0u, p_cost + 1u);
+        warp_append_chunks(ctxs, x_qi[x], nch, u, c_gi, p_cost, 0u, split);
       }
     }
+    __syncwarp();
   }
   // Queries whose distances are final (PH_PREP): one pass over the distance rows
   // gives the star bound min_v sum_i d_i(v) (the cost of the k shortest paths from

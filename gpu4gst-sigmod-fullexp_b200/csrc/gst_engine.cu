@@ -53,6 +53,7 @@ struct SlotMem {
   uint64_t* table = nullptr;
   uint32_t* dist = nullptr;
   uint32_t* rowbits = nullptr;
+  uint32_t* fm[2] = {nullptr, nullptr};
   uint32_t* tour = nullptr;
   uint4* q[2] = {nullptr, nullptr};
   uint4* far[2] = {nullptr, nullptr};
@@ -80,6 +81,8 @@ size_t carve_slot(SlotMem& m, unsigned char* base, int64_t V, size_t rw, uint32_
   m.table = (uint64_t*)take((size_t)V * rw * 8);
   m.dist = (uint32_t*)take((size_t)V * DIST_STRIDE * 4);
   m.rowbits = (uint32_t*)take(((size_t)V + 31) / 32 * 4);
+  m.fm[0] = (uint32_t*)take(((size_t)V + 3) / 4 * 4);
+  m.fm[1] = (uint32_t*)take(((size_t)V + 3) / 4 * 4);
   m.tour = (uint32_t*)take(kTourWords * 4);
   m.q[0] = (uint4*)take((size_t)cap * 16);
   m.q[1] = (uint4*)take((size_t)cap * 16);
@@ -470,6 +473,8 @@ struct Runner {
     c.table = m.table;
     c.dist = m.dist;
     c.rowbits = m.rowbits;
+    c.fm[0] = m.fm[0];
+    c.fm[1] = m.fm[1];
     c.tour = m.tour;
     c.q[0] = m.q[0];
     c.q[1] = m.q[1];
@@ -508,6 +513,8 @@ struct Runner {
     c.far_min = 0xFFFFFFFFu;
     // the hop-limited search runs one round per step, in one cost bucket
     c.bucket_end = c.delta && !c.sssp_hops ? c.delta : 0xFFFFFFFFu;
+    // unlimited distances in one bucket: one distance-search item per (vertex, groups)
+    c.sssp_mask = !c.sssp_hops && c.bucket_end == 0xFFFFFFFFu;
     c.ub = 0xFFFFFFFFu;
     c.cut = 0xFFFFFFFFu;
     c.ub_cell = 0xFFFFFFFFu;
@@ -517,6 +524,10 @@ struct Runner {
     CK(cudaMemsetAsync(m.table, 0xFF, (size_t)g->V * (size_t)c.RW * 8, st));
     CK(cudaMemsetAsync(m.rowbits, 0, ((size_t)g->V + 31) / 32 * 4, st));
     if (c.use_lb) CK(cudaMemsetAsync(m.dist, 0xFF, (size_t)g->V * DIST_STRIDE * 4, st));
+    if (c.sssp_mask) {
+      CK(cudaMemsetAsync(m.fm[0], 0, ((size_t)g->V + 3) / 4 * 4, st));
+      CK(cudaMemsetAsync(m.fm[1], 0, ((size_t)g->V + 3) / 4 * 4, st));
+    }
     CK(cudaMemcpyAsync(d_ctx + s, &c, sizeof(Ctx), cudaMemcpyHostToDevice, st));
     cs.h2d += sizeof(Ctx) + sizeof(int32_t) * q->k;
     const DevGraph G = dev_graph(g);
