@@ -834,6 +834,14 @@ __global__ void __launch_bounds__(256, 3) k_grow(Ctx* ctxs, int nctx, DevGraph G
         ok[x] = j < tot && in_bounds(ctxs + x_qi[x], o_eb + off < G.E, 6);
         ed[x] = ok[x] ? G.wedges[o_eb + off] : make_int2(0, 0);
       }
+      // The bounds are tested before the target's cell is read: an improving target
+      // state (u, X) that cannot be part of a tree within the bound is not written
+      // at all (its cost plus the one-label bound max_{i not in X} d_i(u), or the
+      // O(k) half of the tour bound, exceeds the bound; the same tests the rows
+      // kernel applies before growing a state).  The distance rows of a query
+      // (32 bytes per vertex) stay in L2 while its state table does not, so the
+      // tests come first and only edges that pass them read a table cell.
+      uint4 da[RELAX_U], db[RELAX_U];
 #pragma unroll
       for (int x = 0; x < RELAX_U; x++) {
         Ctx* c = ctxs + x_qi[x];
@@ -841,73 +849,66 @@ __global__ void __launch_bounds__(256, 3) k_grow(Ctx* ctxs, int nctx, DevGraph G
         // a target costing more than ub cannot be part of an optimal tree
         const int hop = c->hop;
         const bool keep = hop ? (nc < x_bound[x]) : (nc <= x_bound[x]);
-        const uint32_t p = x_pd[x] & 0xFFFFu, d = (x_pd[x] >> 16) + (uint32_t)hop;
+        const uint32_t d = (x_pd[x] >> 16) + (uint32_t)hop;
         ok[x] = ok[x] && in_bounds(c, u < G.V, 7) && keep && in_bounds(c, d < (uint32_t)c->DD, 11);
-        cur[x] = ok[x] ? __ldcg((const unsigned long long*)&c->table[(uint64_t)u * c->RW +
-                                                                     ((uint64_t)d << c->k) + p])
-                       : 0ull;
-      }
-      // An improving target state (u, X) that cannot be part of a tree within the
-      // bound is not written at all: its cost plus the one-label bound
-      // max_{i not in X} d_i(u) already exceeds the bound (the same test the rows
-      // kernel applies before growing a state, here before it dirties a row).
-      uint4 da[RELAX_U], db[RELAX_U];
-#pragma unroll
-      for (int x = 0; x < RELAX_U; x++) {
-        Ctx* c = ctxs + x_qi[x];
-        const uint32_t u = (uint32_t)ed[x].x, nc = x_cost[x] + (uint32_t)ed[x].y;
-        ok[x] = ok[x] && pack_cell(nc, PEND | x_v[x]) < cur[x];
         da[x] = db[x] = make_uint4(0, 0, 0, 0);
         if (ok[x] && c->use_lb) {
           const uint4* row = (const uint4*)&c->dist[(uint64_t)u * DIST_STRIDE];
           da[x] = __ldcg(row);
-          db[x] = __ldcg(row + 1);
+          if (c->k > 4) db[x] = __ldcg(row + 1);
         }
       }
 #pragma unroll
       for (int x = 0; x < RELAX_U; x++) {
         Ctx* c = ctxs + x_qi[x];
         const uint32_t u = (uint32_t)ed[x].x, nc = x_cost[x] + (uint32_t)ed[x].y;
-        bool dirty = false;
-        if (ok[x]) {
-          const uint32_t p = x_pd[x] & 0xFFFFu, d = (x_pd[x] >> 16) + (uint32_t)c->hop;
-          if (c->use_lb) {
-            const uint32_t cut = c->cut;
-            const uint32_t lim = cut == COST_INF ? COST_INF : cut + 1u;
-            const uint32_t dd[8] = {da[x].x, da[x].y, da[x].z, da[x].w,
-                                    db[x].x, db[x].y, db[x].z, db[x].w};
-            const int k = c->k;
-            uint32_t lb = 0;
+        const uint32_t p = x_pd[x] & 0xFFFFu, d = (x_pd[x] >> 16) + (uint32_t)c->hop;
+        if (ok[x] && c->use_lb) {
+          const uint32_t cut = c->cut;
+          const uint32_t lim = cut == COST_INF ? COST_INF : cut + 1u;
+          const uint32_t dd[8] = {da[x].x, da[x].y, da[x].z, da[x].w,
+                                  db[x].x, db[x].y, db[x].z, db[x].w};
+          const int k = c->k;
+          uint32_t lb = 0;
+#pragma unroll
+          for (int i = 0; i < KMAX; i++)
+            if (i < k && !((p >> i) & 1u)) lb = max(lb, min(dd[i], lim));
+          if ((uint64_t)nc + lb > (uint64_t)x_bound[x]) ok[x] = false;
+          if (ok[x] && c->use_tour && p != (uint32_t)c->full) {
+            // the O(k) half of the tour bound (see the rows kernel): twice the rest
+            // of any tree holding (u, p) costs at least
+            // max_a d_a(u) + min_b P(a,b,Xb) + min_b d_b(u) over groups a, b not in p
+            const uint32_t Xb = (uint32_t)c->full ^ p;
+            const uint32_t* W2 = c->tour + (size_t)c->W * TOUR_STRIDE + (size_t)Xb * KMAX;
+            uint32_t mind = COST_INF;
 #pragma unroll
             for (int i = 0; i < KMAX; i++)
-              if (i < k && !((p >> i) & 1u)) lb = max(lb, min(dd[i], lim));
-            if ((uint64_t)nc + lb > (uint64_t)x_bound[x]) ok[x] = false;
-            if (ok[x] && c->use_tour && p != (uint32_t)c->full) {
-              // the O(k) half of the tour bound (see the rows kernel): twice the rest
-              // of any tree holding (u, p) costs at least
-              // max_a d_a(u) + min_b P(a,b,Xb) + min_b d_b(u) over groups a, b not in p
-              const uint32_t Xb = (uint32_t)c->full ^ p;
-              const uint32_t* W2 = c->tour + (size_t)c->W * TOUR_STRIDE + (size_t)Xb * KMAX;
-              uint32_t mind = COST_INF;
+              if (i < k && ((Xb >> i) & 1u)) mind = min(mind, min(dd[i], lim));
+            uint64_t lb2 = 0;
 #pragma unroll
-              for (int i = 0; i < KMAX; i++)
-                if (i < k && ((Xb >> i) & 1u)) mind = min(mind, min(dd[i], lim));
-              uint64_t lb2 = 0;
+            for (int i = 0; i < KMAX; i++)
+              if (i < k && ((Xb >> i) & 1u)) {
+                const uint64_t t2 = (uint64_t)min(dd[i], lim) + __ldg(&W2[i]) + mind;
+                lb2 = t2 > lb2 ? t2 : lb2;
+              }
+            if ((uint64_t)nc + (lb2 + 1) / 2 > (uint64_t)x_bound[x]) ok[x] = false;
+          }
+        }
+        cur[x] = ok[x] ? __ldcg((const unsigned long long*)&c->table[(uint64_t)u * c->RW +
+                                                                     ((uint64_t)d << c->k) + p])
+                       : 0ull;
+      }
 #pragma unroll
-              for (int i = 0; i < KMAX; i++)
-                if (i < k && ((Xb >> i) & 1u)) {
-                  const uint64_t t2 = (uint64_t)min(dd[i], lim) + __ldg(&W2[i]) + mind;
-                  lb2 = t2 > lb2 ? t2 : lb2;
-                }
-              if ((uint64_t)nc + (lb2 + 1) / 2 > (uint64_t)x_bound[x]) ok[x] = false;
-            }
-          }
-          if (ok[x]) {
-            unsigned long long* tp =
-                (unsigned long long*)&c->table[(uint64_t)u * c->RW + ((uint64_t)d << c->k) + p];
-            const uint64_t old = atomicMin(tp, (unsigned long long)pack_cell(nc, PEND | x_v[x]));
-            dirty = cost_of(old) > nc;
-          }
+      for (int x = 0; x < RELAX_U; x++) {
+        Ctx* c = ctxs + x_qi[x];
+        const uint32_t u = (uint32_t)ed[x].x, nc = x_cost[x] + (uint32_t)ed[x].y;
+        bool dirty = false;
+        if (ok[x] && pack_cell(nc, PEND | x_v[x]) < cur[x]) {
+          const uint32_t p = x_pd[x] & 0xFFFFu, d = (x_pd[x] >> 16) + (uint32_t)c->hop;
+          unsigned long long* tp =
+              (unsigned long long*)&c->table[(uint64_t)u * c->RW + ((uint64_t)d << c->k) + p];
+          const uint64_t old = atomicMin(tp, (unsigned long long)pack_cell(nc, PEND | x_v[x]));
+          dirty = cost_of(old) > nc;
         }
         warp_mark_row(ctxs, x_qi[x], dirty, u);
       }
