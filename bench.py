@@ -19,9 +19,10 @@ value   : queries/s over the K timed steps, device time (CUDA events on the
 e2e     : the same steps timed on the host around the C-ABI call, which uploads
           each query from host memory and copies every result (cost + tree
           edges) back; the bytes moved are counted by the engine.
-roofline: the grow kernel (dominant launch): algorithmic bytes
-          24 B x work items + 16 B x edge relaxations, over its event-timed
-          duration in the timed region, against the measured HBM copy bandwidth.
+roofline: the level kernel with the most device time in a replay of the first
+          timed batches with CUDA events around every level launch: its algorithmic
+          bytes (level_bytes: per relaxation, work item and merged row) over its
+          event-timed duration, against the measured HBM copy bandwidth.
 cpu_baseline: the reference's own TrimCDP-multi-core-CPU (oracle/_ref, built from
           its sources, all host threads up to its own cap of 100) on a ~20 s sample
           of the same queries.  Its single-thread PrunedDP++ needs about a minute per
@@ -293,17 +294,20 @@ def run_reference_arm(args):
     return 0
 
 
-def level_bytes(answers, queries, hops):
+def level_bytes(answers, queries, hops, bucket_delta=0):
     """Algorithmic bytes of the three level kernels for a set of answered queries:
-    sssp 16 B per relaxation (8 B edge + 4 B distance read + 4 B written); grow
-    24 B per work item (16 B item + 8 B source cell) + 16 B per relaxation (8 B
-    edge + 8 B target cell); rows 16 B per cell of every row merged (the row read
-    once and written back once)."""
+    sssp per relaxation 8 B edge + the target's k distances (4k B) when the search
+    runs group-mask items (unbounded or D = 0 queries in one cost bucket: one
+    relaxation serves all of the item's groups), else 16 B (8 B edge + 4 B distance
+    read + 4 B written); grow 24 B per work item (16 B item + 8 B source cell) +
+    16 B per relaxation (8 B edge + 8 B target cell); rows 16 B per cell of every
+    row merged (the row read once and written back once)."""
     b = {"k_sssp": 0.0, "k_grow": 0.0, "k_rows": 0.0}
     for a, q, h in zip(answers, queries, hops):
         st = a.stats
         rw = (1 << len(q)) * (1 if h is None else h + 1)
-        b["k_sssp"] += 16.0 * st["sssp_relaxations"]
+        masked = (h is None or h == 0) and bucket_delta == 0
+        b["k_sssp"] += (8.0 + 4.0 * len(q) if masked else 16.0) * st["sssp_relaxations"]
         b["k_grow"] += 24.0 * st["states_expanded"] + 16.0 * st["edge_relaxations"]
         b["k_rows"] += 16.0 * rw * st["rows_merged"]
     return b
@@ -457,7 +461,7 @@ def run_ours(args):
         kms["k_grow"] += st["grow_ms"]
         kms["k_rows"] += st["rows_ms"]
         kms["k_sssp"] += st["sssp_ms"]
-        for kname, v in level_bytes(ans, qs, hs).items():
+        for kname, v in level_bytes(ans, qs, hs, tuned["bucket_delta"] if tuned else 0).items():
             kbytes[kname] += v
         for kname, field in (("k_grow", "grow_launches"), ("k_rows", "rows_launches"),
                              ("k_sssp", "sssp_launches")):

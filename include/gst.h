@@ -58,7 +58,9 @@ typedef struct gst_server gst_server;
 typedef struct gst_config {
   int64_t mem_budget_bytes;   /* HBM the engine may use for query state; 0 = 85% of free */
   int32_t split_degree;       /* edges per grow work item: hubs split into chunks of this size */
-  int32_t bucket_delta;       /* cost-bucket width of the frontier ordering; 0 = autotune */
+  int32_t bucket_delta;       /* cost-bucket width of the frontier ordering; 0 = one bucket
+                                 (no ordering; the distance search of unbounded queries then
+                                 runs one item per vertex and group mask) */
   int32_t max_levels;         /* per-query level budget (GST_TIMEOUT beyond) */
   int32_t threads_per_block;  /* CTA size of the rows (merge) kernel, 64..256 */
   int32_t blocks_per_sm;      /* resident CTAs per SM for the level kernels */
