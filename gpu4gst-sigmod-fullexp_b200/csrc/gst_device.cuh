@@ -189,6 +189,29 @@ __device__ __forceinline__ uint32_t deposit(uint32_t b, uint32_t mask) {
   return r;
 }
 
+// Submask table for masks of up to 8 bits: SUBMASK.v[M][b] = deposit(b, M) (the bits
+// of b placed into the set bits of M, lowest first), built at compile time, so that
+// the merge loop enumerates the submasks of a complement with one cached load.
+struct SubmaskTable {
+  unsigned char v[256][256];
+};
+constexpr SubmaskTable make_submask_table() {
+  SubmaskTable t{};
+  for (int M = 0; M < 256; M++)
+    for (int b = 0; b < 256; b++) {
+      int r = 0, bb = b, mm = M;
+      while (mm) {
+        const int low = mm & -mm;
+        if (bb & 1) r |= low;
+        bb >>= 1;
+        mm ^= low;
+      }
+      t.v[M][b] = (unsigned char)r;
+    }
+  return t;
+}
+__device__ const SubmaskTable SUBMASK = make_submask_table();
+
 // x / y for x < 2^22 and 1 <= y, from a float estimate and one correction each way
 // (inv = 1.0f / y computed once by the caller).
 __device__ __forceinline__ uint32_t udiv_small(uint32_t x, uint32_t y, float inv) {
@@ -850,6 +873,7 @@ __global__ void __launch_bounds__(256, 3) k_grow(Ctx* ctxs, int nctx, DevGraph G
         const int hop = c->hop;
         const bool keep = hop ? (nc < x_bound[x]) : (nc <= x_bound[x]);
         const uint32_t d = (x_pd[x] >> 16) + (uint32_t)hop;
+        (void)d;  // only the checked build tests it
         ok[x] = ok[x] && in_bounds(c, u < G.V, 7) && keep && in_bounds(c, d < (uint32_t)c->DD, 11);
         da[x] = db[x] = make_uint4(0, 0, 0, 0);
         if (ok[x] && c->use_lb) {
@@ -1041,7 +1065,7 @@ __global__ void __launch_bounds__(256, 4) k_rows(Ctx* ctxs, int nctx, DevGraph G
           } else {
             // r = d2 * m + (yb - 1): partner hop d2, partner = yb-th submask of ~X
             d2 = udiv_small(r, m, inv_m);
-            Y = deposit(r - d2 * m + 1u, full ^ X);
+            Y = __ldg(&SUBMASK.v[full ^ X][r - d2 * m + 1u]);
           }
           const uint32_t yi = (d2 << k) + Y;
           const uint32_t cy = (Y & X) ? COST_INF : cost_of(buf[yi]);
@@ -1142,37 +1166,56 @@ __global__ void __launch_bounds__(256, 4) k_rows(Ctx* ctxs, int nctx, DevGraph G
       // tour bound of PrunedDP++ (code/PrunedDP++/include/CPUNONHOP.h:433-493): the
       // rest of the tree, doubled, is a closed walk from v through every group of
       // Xb = full \ p, so twice its cost is at least
-      //   min_{a,b} d_a(v) + P(a,b,Xb) + d_b(v)          and, for every a,
-      //   d_a(v) + min_b P(a,b,Xb) + min_b d_b(v),
+      //   lb2 = max_a d_a(v) + min_b P(a,b,Xb) + min_b d_b(v)    and
+      //   lb1 = min_{a,b} d_a(v) + P(a,b,Xb) + d_b(v),
       // P = cheapest group sequence from a to b visiting each group of Xb once.
-      // One candidate at a time, the warp's lanes over the (a, b) pairs.
-      const int a0 = lane >> 3, bb = lane & 7;
-      const uint32_t dla = min(__shfl_sync(0xffffffffu, mine, a0), lim);
-      const uint32_t dla2 = min(__shfl_sync(0xffffffffu, mine, a0 + 4), lim);
-      const uint32_t dlb = min(__shfl_sync(0xffffffffu, mine, bb), lim);
+      // One candidate per lane: the O(k) bound first, the O(k^2) one for the
+      // candidates it keeps (the test is cost + ceil(max(lb1, lb2) / 2) > bound).
       const uint32_t bound = hop ? __ldcg(&c->ub_cell) : __ldcg(&c->ub);
-      for (int t = 0; t < ncand; t++) {
-        const uint32_t i = list[t];
-        const uint32_t p = i & full, cst = cost_of(buf[i]);
-        const uint32_t Xb = full ^ p;
-        const uint32_t* Wt = c->tour + (size_t)Xb * TOUR_STRIDE;
-        const uint32_t* W2 = c->tour + (size_t)c->W * TOUR_STRIDE + (size_t)Xb * KMAX;
-        const bool inA = a0 < k && ((Xb >> a0) & 1u);
-        const bool inA2 = a0 + 4 < k && ((Xb >> (a0 + 4)) & 1u);
-        const bool inB = bb < k && ((Xb >> bb) & 1u);
-        uint64_t t1 = ~0ull;
-        if (inA && inB) t1 = (uint64_t)dla + __ldg(&Wt[a0 * KMAX + bb]) + dlb;
-        if (inA2 && inB) t1 = min(t1, (uint64_t)dla2 + __ldg(&Wt[(a0 + 4) * KMAX + bb]) + dlb);
-        const uint32_t lb1 = __reduce_min_sync(0xffffffffu, (uint32_t)min(t1, (uint64_t)COST_INF));
-        const uint32_t mind = __reduce_min_sync(0xffffffffu, (lane < 8 && inB) ? dlb : COST_INF);
-        uint64_t t2 = 0;
-        if (lane < 8 && inB) t2 = (uint64_t)dlb + __ldg(&W2[bb]) + mind;
-        const uint32_t lb2 = __reduce_max_sync(0xffffffffu, (uint32_t)min(t2, (uint64_t)COST_INF));
-        const uint64_t tb = lb1 > lb2 ? lb1 : lb2;
-        if ((uint64_t)cst + (tb + 1) / 2 > (uint64_t)bound && lane == 0)
-          pend[i >> 5] &= ~(1u << (i & 31));
-        __syncwarp();
+      const uint32_t* tour = c->tour;
+      const uint32_t Wq = (uint32_t)c->W;
+      for (int t0 = 0; t0 < ncand; t0 += 32) {
+        const int t = t0 + lane;
+        if (t < ncand) {
+          const uint32_t i = list[t];
+          const uint32_t p = i & full, cst = cost_of(buf[i]);
+          const uint32_t Xb = full ^ p;
+          const uint32_t* W2 = tour + (size_t)Wq * TOUR_STRIDE + (size_t)Xb * KMAX;
+          uint32_t mind = COST_INF;
+#pragma unroll
+          for (int b2 = 0; b2 < KMAX; b2++)
+            if (b2 < k && ((Xb >> b2) & 1u)) mind = min(mind, dl[b2]);
+          uint64_t lb2 = 0;
+#pragma unroll
+          for (int b2 = 0; b2 < KMAX; b2++)
+            if (b2 < k && ((Xb >> b2) & 1u)) {
+              const uint64_t t2 = (uint64_t)dl[b2] + __ldg(&W2[b2]) + mind;
+              lb2 = t2 > lb2 ? t2 : lb2;
+            }
+          // both bounds saturate at COST_INF (an unreachable group)
+          lb2 = lb2 < COST_INF ? lb2 : COST_INF;
+          bool drop = (uint64_t)cst + (lb2 + 1) / 2 > (uint64_t)bound;
+          if (!drop) {
+            const uint32_t* Wt = tour + (size_t)Xb * TOUR_STRIDE;
+            uint64_t lb1 = ~0ull;
+#pragma unroll
+            for (int a1 = 0; a1 < KMAX; a1++)
+              if (a1 < k && ((Xb >> a1) & 1u)) {
+#pragma unroll
+                for (int b1 = 0; b1 < KMAX; b1++)
+                  if (b1 < k && ((Xb >> b1) & 1u)) {
+                    const uint64_t t1 =
+                        (uint64_t)dl[a1] + __ldg(&Wt[a1 * KMAX + b1]) + dl[b1];
+                    lb1 = t1 < lb1 ? t1 : lb1;
+                  }
+              }
+            lb1 = lb1 < COST_INF ? lb1 : COST_INF;
+            drop = (uint64_t)cst + (lb1 + 1) / 2 > (uint64_t)bound;
+          }
+          if (drop) atomicAnd(&pend[i >> 5], ~(1u << (i & 31)));
+        }
       }
+      __syncwarp();
     }
     // emit the growing states, each relaxed from its lightest edge on (which lands
     // at cst + 1 or later): one reservation per list for the whole row

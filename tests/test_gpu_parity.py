@@ -124,3 +124,45 @@ def test_cost_buckets_match_reference(delta):
         dg.close()
     finally:
         eng.close()
+
+
+def test_overlapping_groups_match_oracle(engine):
+    """Groups that share member vertices: a vertex that starts the distance search
+    for several queried groups at once (several frontier bits set by one launch),
+    and groups nested in others.  Unbounded queries (group-mask distance items),
+    D = 0 (a single-vertex tree or none) and hop-bounded ones (group items) in one
+    batch, against the oracle and against each query solved alone."""
+    rng = np.random.default_rng(41)
+    g = G.synth_rmat(2500, 12000, 42)
+    base = [rng.choice(g.V, size=int(rng.integers(2, 30)), replace=False) for _ in range(12)]
+    lists = []
+    for i, m in enumerate(base):
+        lists.append(sorted(set(m.tolist())))
+        # a group sharing half of its members with the previous one, and a subset
+        other = base[i - 1]
+        lists.append(sorted(set(m[: len(m) // 2].tolist()) | set(other[: len(other) // 2].tolist())))
+        lists.append(sorted(set(m[:1].tolist())))
+    grp = G.Groups.from_lists(lists)
+    dg = engine.graph(g, grp)
+    qs, hops, want = [], [], []
+    for t in range(24):
+        k = int(rng.integers(1, 7))
+        q = rng.choice(len(lists), size=k, replace=False).astype(np.int32)
+        hop = [None, None, 0, 2, 3][t % 5]
+        if t % 10 == 2:
+            # three groups sharing one vertex: a zero-cost tree, for D = 0 and unbounded
+            i = int(rng.integers(0, len(base)))
+            q = np.array([3 * i, 3 * i + 1, 3 * i + 2], dtype=np.int32)
+            hop = 0 if t % 20 == 2 else None
+        o = O.gst_nonhop(g, grp, q) if hop is None else O.gst_hop(g, grp, q, hop)
+        qs.append(q)
+        hops.append(hop)
+        want.append(o["cost"])
+    alone = [dg.solve(q, h) for q, h in zip(qs, hops)]
+    mixed = dg.solve_batch(qs, hops)
+    try:
+        for q, h, a, b, c in zip(qs, hops, alone, mixed, want):
+            _check(g, grp, q, h, a, c)
+            _check(g, grp, q, h, b, c)
+    finally:
+        dg.close()
