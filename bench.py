@@ -297,16 +297,16 @@ def run_reference_arm(args):
 def level_bytes(answers, queries, hops, bucket_delta=0):
     """Algorithmic bytes of the three level kernels for a set of answered queries:
     sssp per relaxation 8 B edge + the target's k distances (4k B) when the search
-    runs group-mask items (unbounded or D = 0 queries in one cost bucket: one
-    relaxation serves all of the item's groups), else 16 B (8 B edge + 4 B distance
-    read + 4 B written); grow 24 B per work item (16 B item + 8 B source cell) +
+    runs group-mask items (hop-bounded queries with D > 0, and every query when the
+    search runs in one cost bucket: one relaxation serves all of the item's groups),
+    else 16 B (8 B edge + 4 B distance read + 4 B written); grow 24 B per work item (16 B item + 8 B source cell) +
     16 B per relaxation (8 B edge + 8 B target cell); rows 16 B per cell of every
     row merged (the row read once and written back once)."""
     b = {"k_sssp": 0.0, "k_grow": 0.0, "k_rows": 0.0}
     for a, q, h in zip(answers, queries, hops):
         st = a.stats
         rw = (1 << len(q)) * (1 if h is None else h + 1)
-        masked = (h is None or h == 0) and bucket_delta == 0
+        masked = (h is not None and h > 0) or bucket_delta == 0
         b["k_sssp"] += (8.0 + 4.0 * len(q) if masked else 16.0) * st["sssp_relaxations"]
         b["k_grow"] += 24.0 * st["states_expanded"] + 16.0 * st["edge_relaxations"]
         b["k_rows"] += 16.0 * rw * st["rows_merged"]

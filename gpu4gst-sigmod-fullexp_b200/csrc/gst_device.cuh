@@ -112,6 +112,8 @@ struct Ctx {
   uint32_t* fm[2];     // group-mask frontier (one byte per vertex, four to a word): the
                        // groups whose distance at the vertex improved in the step that
                        // wrote fm[no]; read and cleared by the next step through fm[in_idx]
+  uint32_t* snap;      // hop-limited group-mask search: the distance rows of a round's
+                       // frontier as they stood when the round began (V x DIST_STRIDE)
   uint32_t* tour;      // 2^k x TOUR_STRIDE path table, then 2^k x KMAX row minima
   uint4* q[2];
   uint4* far[2];
@@ -144,8 +146,9 @@ struct Ctx {
                         // prune against their own, larger, bound and want more of them)
   uint32_t sssp_hops;   // 0: distances d_i(v); D: hop-limited distances d_i^{<=D}(v), the
                         // cheapest paths of at most D edges (hop-bounded queries)
-  uint32_t sssp_mask;   // 1: the distance search runs one item per (vertex, group mask)
-                        // (unlimited distances in one cost bucket); 0: one per (vertex, group)
+  uint32_t sssp_mask;   // distance search items: 0 one per (vertex, group); 1 one per
+                        // (vertex, group mask), unlimited distances in one cost bucket;
+                        // 2 the same for hop-limited distances, one round per two steps
   uint32_t ub_cell;     // best full-state cell
   unsigned long long best;  // cost<<32 | d<<27 | v of the best full-state cell
   uint32_t phase;
@@ -504,7 +507,7 @@ __global__ void k_init(Ctx* ctxs, int nctx, DevGraph G, const int64_t* grp_ptr,
           const uint32_t old = atomicMin(&c->dist[(uint64_t)v * DIST_STRIDE + i], 0u);
           const int64_t deg = G.beg[v + 1] - G.beg[v];
           if (old != 0u && deg > 0 && c->sssp_mask) {
-            // group-mask items: one head item per vertex, the groups in fm
+            // group-mask items: one head item per vertex (hop count 0), the groups in fm
             const uint32_t sh = (v & 3u) * 8u;
             const uint32_t ow = atomicOr(&c->fm[c->no][v >> 2], (1u << i) << sh);
             if (((ow >> sh) & 0xFFu) == 0u) {
@@ -513,16 +516,10 @@ __global__ void k_init(Ctx* ctxs, int nctx, DevGraph G, const int64_t* grp_ptr,
               else atomicOr(&c->error, (uint32_t)ERR_QCAP);
             }
           } else if (old != 0u && deg > 0) {
-            // unlimited distances: one head item; hop-limited: every chunk at once,
-            // so that all edges of a round are relaxed in the same step
-            const uint32_t nch =
-                c->sssp_hops ? (uint32_t)((deg + split - 1) / split) : 1u;
-            const uint32_t pd = c->sssp_hops ? ((uint32_t)i | CHUNK) : (uint32_t)i;
-            const uint32_t n = atomicAdd(&c->n_q[c->no], nch);
-            for (uint32_t j = 0; j < nch; j++) {
-              if (n + j < c->qcap) c->q[c->no][n + j] = make_uint4(v, pd, 0u, j * (uint32_t)split);
-              else atomicOr(&c->error, (uint32_t)ERR_QCAP);
-            }
+            // group items: one head item per (member, group)
+            const uint32_t n = atomicAdd(&c->n_q[c->no], 1u);
+            if (n < c->qcap) c->q[c->no][n] = make_uint4(v, (uint32_t)i, 0u, 0u);
+            else atomicOr(&c->error, (uint32_t)ERR_QCAP);
           }
         }
       }
@@ -534,16 +531,20 @@ __global__ void k_init(Ctx* ctxs, int nctx, DevGraph G, const int64_t* grp_ptr,
 // Two item forms (code/TrimCDP-WB/include/mapper_enactor.cuh:249-366 computes the
 // same distances as grow-only DP states (v, 1<<i)):
 //  - group items {v, group index i [| hops << 8], dist, offset}: relax d_i(u) for the
-//    edges of the item (hop-limited searches, and searches in cost buckets);
-//  - group-mask items (sssp_mask, unlimited distances in one bucket): a head item
-//    {v, 0, 0, 0} takes the groups whose d_i(v) improved in the previous step from
-//    fm[in_idx] (and clears them); a chunk item {v, mask | CHUNK, 0, offset} carries
-//    its groups.  Each edge is read once for all of the item's groups and the
-//    target's 32-byte distance row once, and a vertex improved for several groups in
-//    one step is queued once.  Items relax with the distances current when they run
-//    (a value at most the one announced), and a distance written in a step is
-//    announced in fm of that step, read only by the next launch, so every write is
-//    visible to the item that its bit schedules.
+//    edges of the item (searches in cost buckets);
+//  - group-mask items (sssp_mask): a head item {v, hops << 8, 0, 0} takes the groups
+//    whose d_i(v) improved in the previous step from fm[in_idx] (and clears them); a
+//    chunk item {v, mask | hops << 8 | CHUNK, 0, offset} carries its groups.  Each
+//    edge is read once for all of the item's groups and the target's 32-byte
+//    distance row once, and a vertex improved for several groups in one step is
+//    queued once.  A distance written in a step is announced in fm of that step,
+//    read only by the next launch, so every write is visible to the item that its
+//    bit schedules.  Unlimited distances (sssp_mask 1) relax with the distances
+//    current when an item runs (a value at most the one announced).  Hop-limited
+//    distances d_i^{<=D} (sssp_mask 2) run level-synchronous rounds of two steps:
+//    the expand step snapshots the rows of the announced vertices and queues all
+//    their chunks, the relax step extends exactly those distances by one edge
+//    (rounds 1..D), so that the result is the same as one item per path.
 constexpr uint32_t SSSP_MASKED = 0x40000000u;  // lane-local flag: a group-mask item
 constexpr int SSSP_U = 2;                      // edges per lane per round of the relax loop
 __global__ void __launch_bounds__(256, 4) k_sssp(Ctx* ctxs, int nctx, DevGraph G, int split) {
@@ -577,15 +578,22 @@ __global__ void __launch_bounds__(256, 4) k_sssp(Ctx* ctxs, int nctx, DevGraph G
       if (c->sssp_mask) {
         if (in_bounds(c, v < G.V, 2)) {
           const int64_t b0 = G.beg[v], b1 = G.beg[v + 1];
+          const bool chunk = (gi & CHUNK) != 0u;
+          const uint32_t hops = (gi >> SSSP_HOP_SHIFT) & 0xFFu;
+          const bool rounds = c->sssp_mask == 2u;
           uint32_t m;
-          if (gi & CHUNK) {
+          if (chunk) {
             m = g;
           } else {
             unsigned char* fb = (unsigned char*)c->fm[c->in_idx] + v;
             m = __ldcg(fb);
             *fb = 0;
           }
-          const uint4* row = (const uint4*)&c->dist[(uint64_t)v * DIST_STRIDE];
+          // a hop-limited round relaxes from the distances its frontier had when the
+          // round began (the snapshot its expand step took), so that a round extends
+          // paths by exactly one edge
+          const uint32_t* src = rounds && chunk ? c->snap : c->dist;
+          const uint4* row = (const uint4*)&src[(uint64_t)v * DIST_STRIDE];
           const uint4 a = __ldcg(row), b = __ldcg(row + 1);
           const uint32_t d[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
           ub = sssp_cutoff(c);
@@ -600,8 +608,21 @@ __global__ void __launch_bounds__(256, 4) k_sssp(Ctx* ctxs, int nctx, DevGraph G
               mk |= 1u << i;
             }
           cost = mind;
-          gi = mk | SSSP_MASKED | ((uint32_t)k << 24);
-          if (mk) P = plan_item(G, v, b0, b1, mind, e.w, ub - mind, bend, split, (e.y & CHUNK) != 0u);
+          gi = mk | (hops << SSSP_HOP_SHIFT) | SSSP_MASKED | ((uint32_t)k << 24);
+          if (rounds && !chunk) {
+            // expand step of a round: snapshot the row, queue every chunk of the range
+            // for the next step, relax nothing (no distance changes in this step)
+            uint4* srow = (uint4*)&c->snap[(uint64_t)v * DIST_STRIDE];
+            srow[0] = a;
+            srow[1] = b;
+            if (mk) {
+              const int64_t cnt = count_upto(G, v, b1 - b0, ub - mind);
+              P.spawn = (uint32_t)((cnt + split - 1) / split);
+            }
+            e_off = 0;
+          } else if (mk) {
+            P = plan_item(G, v, b0, b1, mind, e.w, ub - mind, bend, split, chunk);
+          }
         }
       } else if (in_bounds(c, v < G.V && g < (uint32_t)c->k, 2)) {
         const int64_t b0 = G.beg[v], b1 = G.beg[v + 1];
@@ -610,11 +631,8 @@ __global__ void __launch_bounds__(256, 4) k_sssp(Ctx* ctxs, int nctx, DevGraph G
         // a one-query launch is an L2 hot spot); a stale, larger ub prunes less
         ub = sssp_cutoff(c);
         bend = c->bucket_end;
-        // not stale, and still able to reach a vertex at distance <= ub.  A hop-
-        // limited item is relaxed even when its vertex has a cheaper distance
-        // since: that distance may use more edges, and the item's own path of
-        // fewer edges can still reach further within the hop limit.
-        if ((cur >= cost || c->sssp_hops) && cost < ub)
+        // not stale, and still able to reach a vertex at distance <= ub
+        if (cur >= cost && cost < ub)
           P = plan_item(G, v, b0, b1, cost, e.w, ub - cost, bend, split, (gi & CHUNK) != 0u);
       }
       gi &= ~CHUNK;
@@ -623,7 +641,7 @@ __global__ void __launch_bounds__(256, 4) k_sssp(Ctx* ctxs, int nctx, DevGraph G
     s_dv[wib][lane][1] = make_uint4(dv[4], dv[5], dv[6], dv[7]);
     __syncwarp();
     warp_append(ctxs, qi, P.push, P.far, v, gi, cost, P.off, P.key);
-    warp_append_chunks(ctxs, qi, P.spawn, v, (gi & SSSP_MASKED) ? (gi & 0xFFu) : gi, cost,
+    warp_append_chunks(ctxs, qi, P.spawn, v, (gi & SSSP_MASKED) ? (gi & 0xFFFFu) : gi, cost,
                        e_off + P.n, split);
     const uint32_t n = P.n;
     const int64_t eb = P.eb;
@@ -676,7 +694,7 @@ __global__ void __launch_bounds__(256, 4) k_sssp(Ctx* ctxs, int nctx, DevGraph G
         const uint32_t u = (uint32_t)ed[x].x, w = (uint32_t)ed[x].y, nd = x_cost[x] + w;
         Ctx* c = ctxs + x_qi[x];
         bool push = false, far = false;
-        uint32_t nch = 0, p_gi = 0, p_cost = 0, c_gi = 0;
+        uint32_t p_gi = 0, p_cost = 0;
         if (ok[x] && (x_gi[x] & SSSP_MASKED)) {
           // group-mask edge: every group of the owner's item whose distance through
           // this edge beats the target's
@@ -708,15 +726,20 @@ __global__ void __launch_bounds__(256, 4) k_sssp(Ctx* ctxs, int nctx, DevGraph G
               if (i < k) sum += cu[i];
             if (sum < (uint64_t)lim) atomicMin(&c->ub, (uint32_t)sum);
           }
+          // a hop-limited round: u's paths of hops + 1 edges extend only while the
+          // bound allows one more edge
+          const uint32_t hops = (x_gi[x] >> SSSP_HOP_SHIFT) & 0xFFu, hl = c->sssp_hops;
+          if (hl && hops + 1u >= hl) ext = 0u;
           if (ext) {
             // announce the improved groups to the next step; the first announcement
             // of u in this step queues it
             const uint32_t sh = (u & 3u) * 8u;
             const uint32_t ow = atomicOr(&c->fm[c->no][u >> 2], ext << sh);
             push = ((ow >> sh) & 0xFFu) == 0u;
+            p_gi = hl ? (hops + 1u) << SSSP_HOP_SHIFT : 0u;
           }
         } else if (ok[x] && nd < ra[x].x) {
-          const uint32_t grp = x_gi[x] & 0xFFu, hops = x_gi[x] >> SSSP_HOP_SHIFT;
+          const uint32_t grp = x_gi[x] & 0xFFu;
           const uint32_t old = atomicMin(&c->dist[(uint64_t)u * DIST_STRIDE + grp], nd);
           if (nd < old) {
             // star bound from tentative distances: the k paths found so far from u
@@ -731,26 +754,15 @@ __global__ void __launch_bounds__(256, 4) k_sssp(Ctx* ctxs, int nctx, DevGraph G
             for (int i = 0; i < KMAX; i++)
               if (i < k) sum += (i == (int)grp) ? nd : d[i];
             if (sum < (uint64_t)x_ub[x]) atomicMin(&c->ub, (uint32_t)sum);
-            if (!c->sssp_hops) {
-              push = nd < x_ub[x];
-              // an improved vertex relaxes its own edges from the lightest one, which
-              // lands at nd + 1 or later: in this bucket or a later one
-              far = (uint64_t)nd + 1u >= c->bucket_end;
-              p_gi = grp;
-              p_cost = nd;
-            } else if (hops + 1u < c->sssp_hops && nd < x_ub[x]) {
-              // hop-limited: the next round relaxes u's edges, all of its chunks in
-              // the same step (one round = one edge more)
-              const int64_t ub0 = G.beg[u], ub1 = G.beg[u + 1];
-              const int64_t cnt = count_upto(G, u, ub1 - ub0, x_ub[x] - nd);
-              nch = (uint32_t)((cnt + split - 1) / split);
-              c_gi = grp | ((hops + 1u) << SSSP_HOP_SHIFT);
-              p_cost = nd;
-            }
+            push = nd < x_ub[x];
+            // an improved vertex relaxes its own edges from the lightest one, which
+            // lands at nd + 1 or later: in this bucket or a later one
+            far = (uint64_t)nd + 1u >= c->bucket_end;
+            p_gi = grp;
+            p_cost = nd;
           }
         }
         warp_append(ctxs, x_qi[x], push, far, u, p_gi, p_cost, 0u, p_cost + 1u);
-        warp_append_chunks(ctxs, x_qi[x], nch, u, c_gi, p_cost, 0u, split);
       }
     }
     __syncwarp();

@@ -54,6 +54,7 @@ struct SlotMem {
   uint32_t* dist = nullptr;
   uint32_t* rowbits = nullptr;
   uint32_t* fm[2] = {nullptr, nullptr};
+  uint32_t* snap = nullptr;
   uint32_t* tour = nullptr;
   uint4* q[2] = {nullptr, nullptr};
   uint4* far[2] = {nullptr, nullptr};
@@ -83,6 +84,7 @@ size_t carve_slot(SlotMem& m, unsigned char* base, int64_t V, size_t rw, uint32_
   m.rowbits = (uint32_t*)take(((size_t)V + 31) / 32 * 4);
   m.fm[0] = (uint32_t*)take(((size_t)V + 3) / 4 * 4);
   m.fm[1] = (uint32_t*)take(((size_t)V + 3) / 4 * 4);
+  m.snap = (uint32_t*)take((size_t)V * DIST_STRIDE * 4);
   m.tour = (uint32_t*)take(kTourWords * 4);
   m.q[0] = (uint4*)take((size_t)cap * 16);
   m.q[1] = (uint4*)take((size_t)cap * 16);
@@ -475,6 +477,7 @@ struct Runner {
     c.rowbits = m.rowbits;
     c.fm[0] = m.fm[0];
     c.fm[1] = m.fm[1];
+    c.snap = m.snap;
     c.tour = m.tour;
     c.q[0] = m.q[0];
     c.q[1] = m.q[1];
@@ -513,8 +516,9 @@ struct Runner {
     c.far_min = 0xFFFFFFFFu;
     // the hop-limited search runs one round per step, in one cost bucket
     c.bucket_end = c.delta && !c.sssp_hops ? c.delta : 0xFFFFFFFFu;
-    // unlimited distances in one bucket: one distance-search item per (vertex, groups)
-    c.sssp_mask = !c.sssp_hops && c.bucket_end == 0xFFFFFFFFu;
+    // one distance-search item per (vertex, groups): hop-limited distances in rounds,
+    // unlimited ones when the search runs in one bucket
+    c.sssp_mask = c.sssp_hops ? 2u : (c.bucket_end == 0xFFFFFFFFu ? 1u : 0u);
     c.ub = 0xFFFFFFFFu;
     c.cut = 0xFFFFFFFFu;
     c.ub_cell = 0xFFFFFFFFu;
