@@ -68,6 +68,7 @@ constexpr int RELAX_U = 4;               // edges per lane per round of the rela
 // group word (group index in bits 0..7).
 constexpr uint32_t SSSP_HOP_SHIFT = 8;
 constexpr int TOUR_STRIDE = KMAX * KMAX;
+constexpr int HOP_BUDGETS_MAX = 7;       // hop budgets of the one-label distances kept
 
 struct DevGraph {
   int64_t V;
@@ -114,6 +115,8 @@ struct Ctx {
                        // wrote fm[no]; read and cleared by the next step through fm[in_idx]
   uint32_t* snap;      // hop-limited group-mask search: the distance rows of a round's
                        // frontier as they stood when the round began (V x DIST_STRIDE)
+  uint32_t* dist_h;    // hop budgets h = 1..nhb: d_i^{<=h}(v), cheapest paths of at most h
+                       // edges (nhb x V x DIST_STRIDE; budget D is dist itself)
   uint32_t* tour;      // 2^k x TOUR_STRIDE path table, then 2^k x KMAX row minima
   uint4* q[2];
   uint4* far[2];
@@ -146,6 +149,7 @@ struct Ctx {
                         // prune against their own, larger, bound and want more of them)
   uint32_t sssp_hops;   // 0: distances d_i(v); D: hop-limited distances d_i^{<=D}(v), the
                         // cheapest paths of at most D edges (hop-bounded queries)
+  int32_t nhb;          // hop budgets kept in dist_h
   uint32_t sssp_mask;   // distance search items: 0 one per (vertex, group); 1 one per
                         // (vertex, group mask), unlimited distances in one cost bucket;
                         // 2 the same for hop-limited distances, one round per two steps
@@ -174,6 +178,26 @@ __device__ __forceinline__ bool in_bounds(Ctx* c, bool ok, uint32_t site) {
 #else
 #define in_bounds(c, ok, site) true
 #endif
+
+// One-label distances of v within the hop budget h of a hop-bounded query: d_i^{<=h}(v),
+// the cheapest paths of at most h edges.  A state of height d (a tree hanging from v
+// whose deepest vertex is d edges below it) reaches every missing group within
+// D - d edges in any tree of diameter <= D that contains it: the path from the deepest
+// vertex to the group runs through v.  So d^{<=D-d} bounds its completion.  Budget 0
+// is the groups' members (distance 0); budgets above the kept ones use d^{<=D}, a
+// smaller and so still valid bound.
+__device__ __forceinline__ void budget_row(const Ctx* c, int64_t V, uint32_t v, int h, uint4& a,
+                                           uint4& b) {
+  const uint32_t* base = c->dist;
+  if (h >= 1 && h <= c->nhb) base = c->dist_h + (uint64_t)(h - 1) * (uint64_t)V * DIST_STRIDE;
+  const uint4* row = (const uint4*)&base[(uint64_t)v * DIST_STRIDE];
+  a = __ldcg(row);
+  b = __ldcg(row + 1);
+  if (h <= 0) {
+    a = make_uint4(a.x ? COST_INF : 0u, a.y ? COST_INF : 0u, a.z ? COST_INF : 0u, a.w ? COST_INF : 0u);
+    b = make_uint4(b.x ? COST_INF : 0u, b.y ? COST_INF : 0u, b.z ? COST_INF : 0u, b.w ? COST_INF : 0u);
+  }
+}
 
 __device__ __forceinline__ uint32_t cost_of(uint64_t c) { return (uint32_t)(c >> 32); }
 __device__ __forceinline__ uint64_t pack_cell(uint32_t cost, uint32_t low) {
@@ -505,6 +529,8 @@ __global__ void k_init(Ctx* ctxs, int nctx, DevGraph G, const int64_t* grp_ptr,
         mark_row(c, v);
         if (c->phase == PH_SSSP) {
           const uint32_t old = atomicMin(&c->dist[(uint64_t)v * DIST_STRIDE + i], 0u);
+          for (int h = 1; h <= c->nhb; h++)
+            c->dist_h[((uint64_t)(h - 1) * (uint64_t)G.V + v) * DIST_STRIDE + i] = 0u;
           const int64_t deg = G.beg[v + 1] - G.beg[v];
           if (old != 0u && deg > 0 && c->sssp_mask) {
             // group-mask items: one head item per vertex (hop count 0), the groups in fm
@@ -713,6 +739,11 @@ __global__ void __launch_bounds__(256, 4) k_sssp(Ctx* ctxs, int nctx, DevGraph G
                 if (ndi < old) {
                   imp |= 1u << i;
                   if (ndi < lim) ext |= 1u << i;
+                  // a path of hops + 1 edges (hop-limited rounds): a candidate for every
+                  // budget from hops + 1 on
+                  for (int h = (int)((x_gi[x] >> SSSP_HOP_SHIFT) & 0xFFu) + 1; h <= c->nhb; h++)
+                    atomicMin(&c->dist_h[((uint64_t)(h - 1) * (uint64_t)G.V + u) * DIST_STRIDE + i],
+                              ndi);
                 }
                 cu[i] = min(ndi, old);
               }
@@ -776,7 +807,11 @@ __global__ void __launch_bounds__(256, 4) k_sssp(Ctx* ctxs, int nctx, DevGraph G
     Ctx* c = ctxs + qi;
     if (c->phase != PH_PREP) continue;
     const int k = c->k;
-    uint32_t best = COST_INF;
+    uint32_t best = COST_INF, best_h = COST_INF;
+    // Hop-bounded queries: a star whose k paths have at most D/2 edges each spans a tree
+    // of diameter <= D (breadth-first from the centre, every vertex lies within D/2
+    // edges of it), so min_v sum_i d_i^{<=D/2}(v) is a feasible cost of the query
+    const int hs = c->hop && c->sssp_hops && c->D / 2 <= c->nhb ? c->D / 2 : -1;
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < G.V;
          v += (int64_t)gridDim.x * blockDim.x) {
       const uint4* row = (const uint4*)&c->dist[(uint64_t)v * DIST_STRIDE];
@@ -787,6 +822,16 @@ __global__ void __launch_bounds__(256, 4) k_sssp(Ctx* ctxs, int nctx, DevGraph G
       for (int i = 0; i < KMAX; i++)
         if (i < k) sum += d[i];
       if (sum < best) best = (uint32_t)sum;
+      if (hs >= 0) {
+        uint4 ha, hb;
+        budget_row(c, G.V, (uint32_t)v, hs, ha, hb);
+        const uint32_t e[8] = {ha.x, ha.y, ha.z, ha.w, hb.x, hb.y, hb.z, hb.w};
+        uint64_t sh = 0;
+#pragma unroll
+        for (int i = 0; i < KMAX; i++)
+          if (i < k) sh += e[i];
+        if (sh < best_h) best_h = (uint32_t)sh;
+      }
 #pragma unroll
       for (int i = 0; i < KMAX; i++)
         if (i < k && d[i] == 0u) {
@@ -796,8 +841,12 @@ __global__ void __launch_bounds__(256, 4) k_sssp(Ctx* ctxs, int nctx, DevGraph G
         }
     }
     best = __reduce_min_sync(0xffffffffu, best);
+    best_h = __reduce_min_sync(0xffffffffu, best_h);
     if ((threadIdx.x & 31) == 0 && best < COST_INF && best < __ldcg(&c->ub))
       atomicMin(&c->ub, best);
+    // ub_cell bounds with strict tests (a state must beat a tree already found), so a
+    // feasible cost that no state holds yet enters it plus one
+    if ((threadIdx.x & 31) == 0 && best_h < COST_INF - 1u) atomicMin(&c->ub_cell, best_h + 1u);
   }
 }
 
@@ -885,13 +934,18 @@ __global__ void __launch_bounds__(256, 3) k_grow(Ctx* ctxs, int nctx, DevGraph G
         const int hop = c->hop;
         const bool keep = hop ? (nc < x_bound[x]) : (nc <= x_bound[x]);
         const uint32_t d = (x_pd[x] >> 16) + (uint32_t)hop;
-        (void)d;  // only the checked build tests it
         ok[x] = ok[x] && in_bounds(c, u < G.V, 7) && keep && in_bounds(c, d < (uint32_t)c->DD, 11);
         da[x] = db[x] = make_uint4(0, 0, 0, 0);
         if (ok[x] && c->use_lb) {
-          const uint4* row = (const uint4*)&c->dist[(uint64_t)u * DIST_STRIDE];
-          da[x] = __ldcg(row);
-          if (c->k > 4) db[x] = __ldcg(row + 1);
+          if (hop && c->sssp_hops) {
+            // the target state has height d: its bounds are the distances within the
+            // hop budget D - d
+            budget_row(c, G.V, u, c->D - (int)d, da[x], db[x]);
+          } else {
+            const uint4* row = (const uint4*)&c->dist[(uint64_t)u * DIST_STRIDE];
+            da[x] = __ldcg(row);
+            if (c->k > 4) db[x] = __ldcg(row + 1);
+          }
         }
       }
 #pragma unroll
@@ -1111,21 +1165,31 @@ __global__ void __launch_bounds__(256, 4) k_rows(Ctx* ctxs, int nctx, DevGraph G
       }
       __syncwarp();
     }
-    // one-label distances of v (non-hop, or hop with use_lb): lane g holds d_g(v).
-    // dv: distances as stored (path lengths, for the one-label upper bound); dl: the
-    // same clamped to cut + 1, lower bounds for the pruning tests
-    uint32_t dv[KMAX], dl[KMAX];
-    uint32_t lim = COST_INF, mine = COST_INF;
+    // one-label distances of v: dv as stored (path lengths, for the one-label upper
+    // bound); hb the lower bounds of the pruning tests, clamped to cut + 1.  For a
+    // hop-bounded query lane L < D + 1 holds the bounds of a state of height L, the
+    // distances within the hop budget D - L; the tests take the row of their state's
+    // height from that lane.
+    uint32_t dv[KMAX], hb[KMAX];
+    uint32_t lim = COST_INF;
 #pragma unroll
-    for (int i = 0; i < KMAX; i++) dv[i] = dl[i] = COST_INF;
+    for (int i = 0; i < KMAX; i++) dv[i] = hb[i] = COST_INF;
+    const bool budgets = c->use_lb && hop && c->sssp_hops;
     if (c->use_lb) {
-      mine = lane < k ? __ldcg(&c->dist[(uint64_t)v * DIST_STRIDE + lane]) : COST_INF;
+      const uint32_t mine = lane < k ? __ldcg(&c->dist[(uint64_t)v * DIST_STRIDE + lane]) : COST_INF;
       const uint32_t cut = c->cut;
       lim = cut == COST_INF ? COST_INF : cut + 1u;
 #pragma unroll
       for (int i = 0; i < KMAX; i++) {
         dv[i] = __shfl_sync(0xffffffffu, mine, i);
-        dl[i] = min(dv[i], lim);
+        hb[i] = min(dv[i], lim);
+      }
+      if (budgets) {
+        uint4 a, b;
+        budget_row(c, G.V, v, D - min(lane, D), a, b);
+        const uint32_t e[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+        for (int i = 0; i < KMAX; i++) hb[i] = min(e[i], lim);
       }
     }
     const int64_t deg = G.beg[v + 1] - G.beg[v];
@@ -1137,6 +1201,15 @@ __global__ void __launch_bounds__(256, 4) k_rows(Ctx* ctxs, int nctx, DevGraph G
     for (int i0 = 0; i0 < RW; i0 += 32) {
       const int i = i0 + lane;
       bool keep = false, cand = false;
+      uint32_t dl[KMAX];
+      if (budgets) {
+        const int src = (i < RW ? i : 0) >> k;  // the lane holding this height's bounds
+#pragma unroll
+        for (int b = 0; b < KMAX; b++) dl[b] = __shfl_sync(0xffffffffu, hb[b], src);
+      } else {
+#pragma unroll
+        for (int b = 0; b < KMAX; b++) dl[b] = hb[b];
+      }
       if (i < RW && ((pend[i >> 5] >> (i & 31)) & 1u)) {
         const uint64_t x = buf[i];
         row[i] = x & ~(uint64_t)PEND;
@@ -1188,6 +1261,15 @@ __global__ void __launch_bounds__(256, 4) k_rows(Ctx* ctxs, int nctx, DevGraph G
       const uint32_t Wq = (uint32_t)c->W;
       for (int t0 = 0; t0 < ncand; t0 += 32) {
         const int t = t0 + lane;
+        uint32_t dl[KMAX];
+        if (budgets) {
+          const int src = t < ncand ? (int)(list[t] >> k) : 0;
+#pragma unroll
+          for (int b = 0; b < KMAX; b++) dl[b] = __shfl_sync(0xffffffffu, hb[b], src);
+        } else {
+#pragma unroll
+          for (int b = 0; b < KMAX; b++) dl[b] = hb[b];
+        }
         if (t < ncand) {
           const uint32_t i = list[t];
           const uint32_t p = i & full, cst = cost_of(buf[i]);

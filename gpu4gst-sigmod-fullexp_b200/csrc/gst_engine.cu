@@ -55,6 +55,8 @@ struct SlotMem {
   uint32_t* rowbits = nullptr;
   uint32_t* fm[2] = {nullptr, nullptr};
   uint32_t* snap = nullptr;
+  uint32_t* dist_h = nullptr;  // hop budgets 1..nhb of the one-label distances
+  int nhb = 0;
   uint32_t* tour = nullptr;
   uint4* q[2] = {nullptr, nullptr};
   uint4* far[2] = {nullptr, nullptr};
@@ -72,7 +74,7 @@ size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 // Lay out (or, with base == nullptr, only size) a slot of V rows of rw cells.
 size_t carve_slot(SlotMem& m, unsigned char* base, int64_t V, size_t rw, uint32_t cap,
-                  uint32_t farcap) {
+                  uint32_t farcap, int nhb) {
   size_t off = 0;
   auto take = [&](size_t n) {
     unsigned char* p = base ? base + off : nullptr;
@@ -85,6 +87,8 @@ size_t carve_slot(SlotMem& m, unsigned char* base, int64_t V, size_t rw, uint32_
   m.fm[0] = (uint32_t*)take(((size_t)V + 3) / 4 * 4);
   m.fm[1] = (uint32_t*)take(((size_t)V + 3) / 4 * 4);
   m.snap = (uint32_t*)take((size_t)V * DIST_STRIDE * 4);
+  m.dist_h = (uint32_t*)take((size_t)nhb * (size_t)V * DIST_STRIDE * 4);
+  m.nhb = nhb;
   m.tour = (uint32_t*)take(kTourWords * 4);
   m.q[0] = (uint4*)take((size_t)cap * 16);
   m.q[1] = (uint4*)take((size_t)cap * 16);
@@ -103,6 +107,10 @@ size_t carve_slot(SlotMem& m, unsigned char* base, int64_t V, size_t rw, uint32_
 }
 
 size_t row_width(int k, int D) { return ((size_t)1 << k) * (size_t)(D >= 0 ? D + 1 : 1); }
+
+// Hop budgets 1..n of the one-label distances kept for a hop bound D (budget D is the
+// distance table itself, budget 0 the group members).
+int hop_budgets(int D) { return D > 1 ? std::min(D - 1, HOP_BUDGETS_MAX) : 0; }
 
 // Worklist capacity.  A level appends at most one item per edge chunk of every
 // state it settles, which in the worst case is every cell of the slab; queries
@@ -239,6 +247,7 @@ struct Job {
   Clock::time_point t_submit;
   int boost = 0;                 // worklist capacity boost (capacity retries)
   size_t rw = 0;
+  int nhb = 0;                   // hop budgets of the one-label distances
   std::atomic<bool> done{false};
 };
 
@@ -336,7 +345,7 @@ struct Runner {
     SlotMem tmp;
     const int split = eng->cfg.split_degree;
     const uint32_t cap = list_cap(g->V, g->E, j.rw, split, j.boost);
-    return carve_slot(tmp, nullptr, g->V, j.rw, cap, eng->cfg.bucket_delta > 0 ? cap : 0);
+    return carve_slot(tmp, nullptr, g->V, j.rw, cap, eng->cfg.bucket_delta > 0 ? cap : 0, j.nhb);
   }
 
   int rw_max() const {
@@ -446,7 +455,7 @@ struct Runner {
     int s = -1;
     for (int i = 0; i < max_slots && s < 0; i++)
       if (!owner[i] && mem[i].base && mem[i].rw >= j->rw && mem[i].cap >= cap &&
-          mem[i].farcap >= farcap)
+          mem[i].farcap >= farcap && mem[i].nhb >= j->nhb)
         s = i;
     if (s < 0) {
       for (int i = 0; i < max_slots && s < 0; i++)
@@ -461,7 +470,7 @@ struct Runner {
       if (st != GST_OK) return st;
       if (!p) return GST_NOT_READY;
       SlotMem m;
-      carve_slot(m, (unsigned char*)p, g->V, j->rw, cap, farcap);
+      carve_slot(m, (unsigned char*)p, g->V, j->rw, cap, farcap, j->nhb);
       m.base = p;
       m.bytes = need;
       mem[s] = m;
@@ -478,6 +487,8 @@ struct Runner {
     c.fm[0] = m.fm[0];
     c.fm[1] = m.fm[1];
     c.snap = m.snap;
+    c.dist_h = m.dist_h;
+    c.nhb = j->nhb;
     c.tour = m.tour;
     c.q[0] = m.q[0];
     c.q[1] = m.q[1];
@@ -532,6 +543,8 @@ struct Runner {
       CK(cudaMemsetAsync(m.fm[0], 0, ((size_t)g->V + 3) / 4 * 4, st));
       CK(cudaMemsetAsync(m.fm[1], 0, ((size_t)g->V + 3) / 4 * 4, st));
     }
+    if (c.nhb)
+      CK(cudaMemsetAsync(m.dist_h, 0xFF, (size_t)c.nhb * (size_t)g->V * DIST_STRIDE * 4, st));
     CK(cudaMemcpyAsync(d_ctx + s, &c, sizeof(Ctx), cudaMemcpyHostToDevice, st));
     cs.h2d += sizeof(Ctx) + sizeof(int32_t) * q->k;
     const DevGraph G = dev_graph(g);
@@ -823,6 +836,7 @@ void make_job(Job& j, const gst_query* q, gst_result* r) {
   j.out = r;
   j.t_submit = Clock::now();
   j.rw = row_width(q->k, q->hop_bound);
+  j.nhb = hop_budgets(q->hop_bound);
 }
 
 }  // namespace
