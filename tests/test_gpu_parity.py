@@ -166,3 +166,32 @@ def test_overlapping_groups_match_oracle(engine):
             _check(g, grp, q, h, b, c)
     finally:
         dg.close()
+
+
+def test_hop_budgets_match_oracle(engine):
+    """Hop-bounded queries over the whole range of bounds: the per-height distance
+    budgets (D - 1 of them up to 7 kept, the rest falling back to the full hop
+    bound), the star of D/2-edge paths as the first bound, D = 1 (budget 0, the
+    members themselves) and D = 0."""
+    rng = np.random.default_rng(77)
+    for trial in range(3):
+        if trial == 1:
+            g = G.synth_ba(1200, 2, 500 + trial)
+        else:
+            g = G.synth_rmat(1500, 7000, 500 + trial)
+        grp = G.synth_groups_zipf(g.V, 80, 1.5, 1, 40, 600 + trial)
+        dg = engine.graph(g, grp)
+        qs, hops, want = [], [], []
+        for D in (0, 1, 2, 3, 5, 6, 9):
+            for k in (2, 4, 6):
+                q = G.synth_queries(grp.n_groups, 1, k, int(rng.integers(1, 1 << 30)))[0]
+                qs.append(q)
+                hops.append(D)
+                want.append(O.gst_hop(g, grp, q, D)["cost"])
+        try:
+            for q, h, c in zip(qs, hops, want):
+                _check(g, grp, q, h, dg.solve(q, h), c)
+            for q, h, a, c in zip(qs, hops, dg.solve_batch(qs, hops), want):
+                _check(g, grp, q, h, a, c)
+        finally:
+            dg.close()
