@@ -154,6 +154,8 @@ struct Ctx {
                         // (vertex, group mask), unlimited distances in one cost bucket;
                         // 2 the same for hop-limited distances, one round per two steps
   uint32_t ub_cell;     // best full-state cell
+  uint32_t ub_hop;      // hop-bounded queries: best star of paths of at most D/2 edges
+                        // found by the distance search (a tree of diameter <= D)
   unsigned long long best;  // cost<<32 | d<<27 | v of the best full-state cell
   uint32_t phase;
   uint32_t error;
@@ -278,9 +280,16 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x) {
 // list under the key cost + weight(next edge), so heavy edges are read only once
 // the frontier has reached their target cost, by which time ub has usually pruned
 // them.  The near list holds items of the current bucket.
-// Distance cutoff of the one-label search: cut_mult x ub, saturating.
+// Distance cutoff of the one-label search: cut_mult x ub, saturating; for hop-limited
+// distances at least the best star of D/2-edge paths, a feasible cost of the query, so
+// that every distance a pruning test can use (up to the query's own bound) is exact.
+// Both terms only decrease, so the cutoff never grows during the search.
 __device__ __forceinline__ uint32_t sssp_cutoff(const Ctx* c) {
-  const uint64_t x = (uint64_t)__ldcg(&c->ub) * (c->cut_mult ? c->cut_mult : 1u);
+  uint64_t x = (uint64_t)__ldcg(&c->ub) * (c->cut_mult ? c->cut_mult : 1u);
+  if (c->sssp_hops) {
+    const uint32_t h = __ldcg(&c->ub_hop);
+    x = x > h ? x : h;
+  }
   return x >= COST_INF ? COST_INF : (uint32_t)x;
 }
 
@@ -756,6 +765,11 @@ __global__ void __launch_bounds__(256, 4) k_sssp(Ctx* ctxs, int nctx, DevGraph G
             for (int i = 0; i < KMAX; i++)
               if (i < k) sum += cu[i];
             if (sum < (uint64_t)lim) atomicMin(&c->ub, (uint32_t)sum);
+            // hop-limited rounds up to D/2: every distance of u comes from a path of at
+            // most D/2 edges, so the star spans a tree of diameter <= D
+            const uint32_t hr = ((x_gi[x] >> SSSP_HOP_SHIFT) & 0xFFu) + 1u;
+            if (c->sssp_hops && 2u * hr <= c->sssp_hops && sum < (uint64_t)__ldcg(&c->ub_hop))
+              atomicMin(&c->ub_hop, (uint32_t)sum);
           }
           // a hop-limited round: u's paths of hops + 1 edges extend only while the
           // bound allows one more edge

@@ -533,6 +533,7 @@ struct Runner {
     c.ub = 0xFFFFFFFFu;
     c.cut = 0xFFFFFFFFu;
     c.ub_cell = 0xFFFFFFFFu;
+    c.ub_hop = 0xFFFFFFFFu;
     c.best = ~0ull;
     c.phase = c.use_lb ? PH_SSSP : PH_DP;
     cudaStream_t st = eng->stream;
@@ -1793,6 +1794,7 @@ gst_status noalloc_solve(int device, cudaStream_t st, int64_t V, int64_t E, cons
   c.ub = 0xFFFFFFFFu;
   c.cut = 0xFFFFFFFFu;
   c.ub_cell = 0xFFFFFFFFu;
+  c.ub_hop = 0xFFFFFFFFu;
   c.best = ~0ull;
   c.phase = c.use_lb ? PH_SSSP : PH_DP;
   Ctx* d_ctx = (Ctx*)base;
