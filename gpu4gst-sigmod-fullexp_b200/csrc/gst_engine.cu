@@ -355,18 +355,24 @@ struct Runner {
     return (int)r;
   }
 
-  // First-fit range of `need` bytes from the arenas, or nullptr.
+  // A range of `need` bytes from the arenas, or nullptr.
   void* arena_take(size_t need) {
+    // best fit: the smallest free range that holds `need`, so that the large ranges
+    // that large slots (k = 7 hop-bounded tables run to 12 GB) leave behind stay whole
+    Arena* ba = nullptr;
+    size_t bi = 0;
     for (auto& a : arenas)
       for (size_t i = 0; i < a.free_.size(); i++)
-        if (a.free_[i].second >= need) {
-          const size_t off = a.free_[i].first;
-          a.free_[i].first += need;
-          a.free_[i].second -= need;
-          if (a.free_[i].second == 0) a.free_.erase(a.free_.begin() + (long)i);
-          return a.base + off;
+        if (a.free_[i].second >= need && (!ba || a.free_[i].second < ba->free_[bi].second)) {
+          ba = &a;
+          bi = i;
         }
-    return nullptr;
+    if (!ba) return nullptr;
+    const size_t off = ba->free_[bi].first;
+    ba->free_[bi].first += need;
+    ba->free_[bi].second -= need;
+    if (ba->free_[bi].second == 0) ba->free_.erase(ba->free_.begin() + (long)bi);
+    return ba->base + off;
   }
   // Return a range to its arena, merging it with free neighbours.
   void arena_give(void* p, size_t n) {
@@ -450,12 +456,13 @@ struct Runner {
     const uint32_t farcap = eng->cfg.bucket_delta > 0 ? cap : 0;
     const size_t need = job_bytes(*j);
     if (need > budget) return GST_OOM_ADMISSION;
-    // the lowest free slot whose memory already fits (low slots keep the contexts
-    // the kernels scan few), else the lowest free slot
+    // the free slot whose memory already fits with the least to spare (a small query
+    // does not take a large slot that a large one will want; among equals the lowest,
+    // which keeps the contexts the kernels scan few), else the lowest free slot
     int s = -1;
-    for (int i = 0; i < max_slots && s < 0; i++)
+    for (int i = 0; i < max_slots; i++)
       if (!owner[i] && mem[i].base && mem[i].rw >= j->rw && mem[i].cap >= cap &&
-          mem[i].farcap >= farcap && mem[i].nhb >= j->nhb)
+          mem[i].farcap >= farcap && mem[i].nhb >= j->nhb && (s < 0 || mem[i].bytes < mem[s].bytes))
         s = i;
     if (s < 0) {
       for (int i = 0; i < max_slots && s < 0; i++)
