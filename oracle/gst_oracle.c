@@ -27,6 +27,9 @@
  *                       (v,p2,d2), d2<=D-d, into max(d,d2) (:205-225), stop at
  *                       the first popped full-set state at any d<=D (:184-188),
  *                       parent walk (:231-257).
+ *   oracle_hop_bound_check  not a reference algorithm: oracle_gst_hop pruned with
+ *                       the engine's hop-bounded bounds, so that tests can check
+ *                       that those bounds never remove an optimal tree.
  *
  * Parity pin: tests/golden/ holds costs produced by the reference's own CPU
  * solvers (compiled unmodified under oracle/_ref by oracle/Makefile) on seeded
@@ -410,5 +413,121 @@ int oracle_gst_hop(int64_t V, const int64_t* beg, const int32_t* adj, const int3
   free(typ);
   free(pa);
   free(pb);
+  return 0;
+}
+
+/* ---- check of the engine's hop-bounded pruning (not a reference algorithm) ----
+ * oracle_hop_bound_check runs the cost-ordered hop DP of oracle_gst_hop, but keeps
+ * no grown or merged state (v, p, d) of cost c with
+ *     c + max_{i not in p} d_i^{<=D-d}(v) > ub,
+ * d^{<=h} being the cheapest paths of at most h edges (h synchronous rounds here)
+ * and ub the cheapest star of paths of at most D/2 edges (a tree of diameter <= D),
+ * or no bound when no such star exists.  These are the bounds the engine's
+ * hop-bounded queries prune with (it keeps c + lb <= ub + 1, a looser test).  The
+ * tests compare the cost with oracle_gst_hop's: equal costs on random instances
+ * check that the bounds never remove an optimal tree.
+ * Outputs: cost (-1 infeasible), star (-1 none), pops (states settled). */
+int oracle_hop_bound_check(int64_t V, const int64_t* beg, const int32_t* adj, const int32_t* w,
+                           const int64_t* grp_ptr, const int32_t* members, int32_t k,
+                           const int32_t* group_ids, int32_t D, int64_t* cost, int64_t* star,
+                           int64_t* pops) {
+  if (k < 1 || k > 16 || D < 0 || D > 64) return 1;
+  const int32_t W = 1 << k, FULL = W - 1, DD = D + 1;
+  const int64_t S = V * W * DD;
+  uint32_t* mask = query_masks(V, grp_ptr, members, k, group_ids);
+  int64_t* dh = (int64_t*)malloc(sizeof(int64_t) * (size_t)(V * k * DD));
+  int64_t* c = (int64_t*)malloc(sizeof(int64_t) * (size_t)S);
+  if (!mask || !dh || !c) return 2;
+  /* d^{<=h}: round h extends the paths of round h - 1 by one edge */
+  for (int64_t v = 0; v < V; v++)
+    for (int32_t i = 0; i < k; i++) dh[v * k + i] = (mask[v] >> i & 1) ? 0 : ORACLE_INF;
+  for (int32_t h = 1; h <= D; h++) {
+    const int64_t* prev = dh + (int64_t)(h - 1) * V * k;
+    int64_t* cur = dh + (int64_t)h * V * k;
+    memcpy(cur, prev, sizeof(int64_t) * (size_t)(V * k));
+    for (int64_t v = 0; v < V; v++)
+      for (int64_t e = beg[v]; e < beg[v + 1]; e++)
+        for (int32_t i = 0; i < k; i++) {
+          const int64_t x = prev[v * k + i] + w[e];
+          if (prev[v * k + i] < ORACLE_INF && x < cur[(int64_t)adj[e] * k + i])
+            cur[(int64_t)adj[e] * k + i] = x;
+        }
+  }
+  int64_t ub = ORACLE_INF;
+  {
+    const int64_t* half = dh + (int64_t)(D / 2) * V * k;
+    for (int64_t v = 0; v < V; v++) {
+      int64_t s = 0;
+      for (int32_t i = 0; i < k && s < ORACLE_INF; i++)
+        s = half[v * k + i] >= ORACLE_INF ? ORACLE_INF : s + half[v * k + i];
+      if (s < ub) ub = s;
+    }
+  }
+  *star = ub < ORACLE_INF ? ub : -1;
+  for (int64_t i = 0; i < S; i++) c[i] = ORACLE_INF;
+  heap_t h = {0};
+#define IDX(v, p, d) (((int64_t)(v) * W + (p)) * DD + (d))
+  /* lower bound of state (v, p, d): the missing groups within the budget D - d */
+#define LB(v, p, d, out)                                                       \
+  do {                                                                         \
+    const int64_t* row_ = dh + ((int64_t)(D - (d)) * V + (v)) * k;             \
+    (out) = 0;                                                                 \
+    for (int32_t i_ = 0; i_ < k; i_++)                                         \
+      if (!((p) >> i_ & 1) && row_[i_] > (out)) (out) = row_[i_];              \
+  } while (0)
+  for (int64_t v = 0; v < V; v++)
+    for (int32_t i = 0; i < k; i++)
+      if (mask[v] >> i & 1) {
+        c[IDX(v, 1 << i, 0)] = 0;
+        hitem it = {0, (int32_t)v, 1 << i, 0};
+        heap_push(&h, it);
+      }
+  int64_t npop = 0, best = -1;
+  while (h.n) {
+    hitem it = heap_pop(&h);
+    const int32_t v = it.v, p = it.p, d = it.d;
+    const int64_t cv = it.key;
+    if (cv != c[IDX(v, p, d)]) continue;
+    npop++;
+    if (p == FULL) {
+      best = cv;
+      break;
+    }
+    if (d < D)
+      for (int64_t e = beg[v]; e < beg[v + 1]; e++) {
+        const int64_t t = IDX(adj[e], p, d + 1), nc = cv + w[e];
+        int64_t lb;
+        LB(adj[e], p, d + 1, lb);
+        if (c[t] > nc && nc + lb <= ub) {
+          c[t] = nc;
+          hitem ni = {nc, adj[e], p, d + 1};
+          heap_push(&h, ni);
+        }
+      }
+    for (int32_t p2 = 1; p2 <= FULL; p2++) {
+      if (p2 & p) continue;
+      for (int32_t d2 = 0; d2 <= D - d; d2++) {
+        const int64_t c2 = c[IDX(v, p2, d2)];
+        if (c2 >= ORACLE_INF) continue;
+        const int32_t nd = d > d2 ? d : d2, q = p | p2;
+        const int64_t t = IDX(v, q, nd), nc = cv + c2;
+        int64_t lb = 0;
+        if (q != FULL) LB(v, q, nd, lb);
+        if (c[t] > nc && nc + lb <= ub) {
+          c[t] = nc;
+          hitem ni = {nc, v, q, nd};
+          heap_push(&h, ni);
+        }
+      }
+    }
+  }
+#undef LB
+#undef IDX
+  *cost = best;
+  *pops = npop;
+  free(h.a);
+  free(mask);
+  free(dh);
+  free(c);
   return 0;
 }

@@ -66,3 +66,33 @@ def test_oracle_sssp_matches_dp_singletons():
     for v in mem:
         for e in range(g.beg_pos[v], g.beg_pos[v + 1]):
             assert d[g.adj[e]] <= g.weight[e]
+
+
+def test_hop_budget_bounds_keep_the_optimum():
+    """The engine prunes hop-bounded states with the distances within each state's
+    remaining hop budget (a state of height d reaches every missing group within
+    D - d edges) against the star of D/2-edge paths.  The DP pruned that way finds
+    the same optimum as the unpruned one on random instances, the star is a
+    feasible cost (never below the optimum), and the pruning settles fewer states."""
+    rng = np.random.default_rng(2024)
+    n = 0
+    for t in range(24):
+        if t % 2:
+            g = G.synth_rmat(int(rng.integers(300, 1500)), int(rng.integers(1500, 8000)),
+                             int(rng.integers(1, 1 << 30)))
+        else:
+            g = G.synth_ba(int(rng.integers(300, 1500)), int(rng.integers(1, 4)),
+                           int(rng.integers(1, 1 << 30)))
+        grp = G.synth_groups_zipf(g.V, 40, 1.5, 1, 30, int(rng.integers(1, 1 << 30)))
+        for _ in range(4):
+            k = int(rng.integers(2, 6))
+            D = int(rng.integers(1, 7))
+            q = G.synth_queries(grp.n_groups, 1, k, int(rng.integers(1, 1 << 30)))[0]
+            plain = O.gst_hop(g, grp, q, D)
+            chk = O.hop_bound_check(g, grp, q, D)
+            assert chk["cost"] == plain["cost"], (t, k, D, chk, plain["cost"])
+            if chk["star"] >= 0:
+                assert plain["cost"] >= 0 and chk["star"] >= plain["cost"]
+            assert chk["pops"] <= plain["pops"]
+            n += 1
+    assert n == 96
