@@ -150,6 +150,9 @@ struct Ctx {
   uint32_t sssp_hops;   // 0: distances d_i(v); D: hop-limited distances d_i^{<=D}(v), the
                         // cheapest paths of at most D edges (hop-bounded queries)
   int32_t nhb;          // hop budgets kept in dist_h
+  uint32_t sssp_full;   // 1: distances exact everywhere (no cutoff): a distance-only job,
+                        // or distances gathered from the group cache
+  uint32_t dist_only;   // 1: a distance-only job (group cache fill): done at PREP
   uint32_t sssp_mask;   // distance search items: 0 one per (vertex, group); 1 one per
                         // (vertex, group mask), unlimited distances in one cost bucket;
                         // 2 the same for hop-limited distances, one round per two steps
@@ -285,6 +288,7 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x) {
 // that every distance a pruning test can use (up to the query's own bound) is exact.
 // Both terms only decrease, so the cutoff never grows during the search.
 __device__ __forceinline__ uint32_t sssp_cutoff(const Ctx* c) {
+  if (c->sssp_full) return COST_INF;
   uint64_t x = (uint64_t)__ldcg(&c->ub) * (c->cut_mult ? c->cut_mult : 1u);
   if (c->sssp_hops) {
     const uint32_t h = __ldcg(&c->ub_hop);
@@ -518,6 +522,23 @@ __device__ __forceinline__ void add_stat(Ctx* ctxs, int qi, bool valid, uint32_t
   const uint32_t tot = __reduce_add_sync(peers, valid && x > 0 ? x : 0u);
   if (valid && x > 0 && lane == __ffs(peers) - 1)
     atomicAdd(&(ctxs[qi].*field), (unsigned long long)tot);
+}
+
+// ---- group cache: distance rows of a query from cached per-group vectors ----------
+struct GroupVecs {
+  const uint32_t* v[KMAX];  // d_i(.) of the query's i-th group, V entries each
+};
+__global__ void k_gather_dist(Ctx* c, GroupVecs gv, int64_t V) {
+  const int k = c->k;
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < V;
+       v += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t d[KMAX];
+#pragma unroll
+    for (int i = 0; i < KMAX; i++) d[i] = i < k ? __ldg(&gv.v[i][v]) : COST_INF;
+    uint4* row = (uint4*)&c->dist[(uint64_t)v * DIST_STRIDE];
+    row[0] = make_uint4(d[0], d[1], d[2], d[3]);
+    row[1] = make_uint4(d[4], d[5], d[6], d[7]);
+  }
 }
 
 // ---- init: group members -> zero-cost singletons, SSSP sources, dirty rows ----
@@ -1474,6 +1495,14 @@ __global__ void k_ctrl(Ctx* ctxs, int nctx, int mode) {
   const int qi = blockIdx.x;
   if (qi >= nctx) return;
   Ctx* c = ctxs + qi;
+  if (mode == CTRL_SSSP && c->phase == PH_PREP && !c->error && c->dist_only) {
+    // a group-cache fill: its distances are final, nothing else to build
+    if (threadIdx.x == 0) {
+      c->phase = PH_DONE;
+      c->in_n = 0;
+    }
+    return;
+  }
   if (mode == CTRL_SSSP && c->phase == PH_PREP && !c->error) {
     // The distances are final up to the cutoff ub: every stored distance <= ub is
     // exact, and any other is only known to be > ub.  The group distances feed a

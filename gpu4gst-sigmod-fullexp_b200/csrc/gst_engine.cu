@@ -164,6 +164,21 @@ struct gst_groups {
   int64_t* d_ptr = nullptr;
   int32_t* d_mem = nullptr;
   std::vector<int64_t> h_ptr;
+  // One-label distance cache: the distances of a group to every vertex depend on the
+  // group only, not on the query, so hot groups keep theirs on the device (V uint32
+  // per cached group, least recently warmed replaced first).
+  struct Cache {
+    uint32_t* d_vec = nullptr;       // cap x V
+    int32_t cap = 0;
+    std::vector<int32_t> slot_of;    // group id -> slot, -1 if not cached
+    std::vector<int32_t> gid_of;     // slot -> group id, -1 if empty
+    std::vector<uint64_t> used;      // slot -> last warm call that listed it
+    uint64_t clock = 0;
+    const uint32_t* vec(int64_t V, int32_t gid) const {
+      const int32_t s = gid >= 0 && gid < (int32_t)slot_of.size() ? slot_of[gid] : -1;
+      return s < 0 ? nullptr : d_vec + (size_t)s * (size_t)V;
+    }
+  } cache;
 };
 
 namespace {
@@ -248,6 +263,8 @@ struct Job {
   int boost = 0;                 // worklist capacity boost (capacity retries)
   size_t rw = 0;
   int nhb = 0;                   // hop budgets of the one-label distances
+  uint32_t* cache_dst = nullptr; // a group-cache fill: the distances of group gids[0] to
+                                 // every vertex go here (V entries), no DP
   std::atomic<bool> done{false};
 };
 
@@ -536,17 +553,33 @@ struct Runner {
     c.bucket_end = c.delta && !c.sssp_hops ? c.delta : 0xFFFFFFFFu;
     // one distance-search item per (vertex, groups): hop-limited distances in rounds,
     // unlimited ones when the search runs in one bucket
-    c.sssp_mask = c.sssp_hops ? 2u : (c.bucket_end == 0xFFFFFFFFu ? 1u : 0u);
     c.ub = 0xFFFFFFFFu;
     c.cut = 0xFFFFFFFFu;
     c.ub_cell = 0xFFFFFFFFu;
     c.ub_hop = 0xFFFFFFFFu;
     c.best = ~0ull;
     c.phase = c.use_lb ? PH_SSSP : PH_DP;
+    // a group-cache fill: the distances of one group, exact everywhere, then done
+    if (j->cache_dst) {
+      c.dist_only = 1;
+      c.sssp_full = 1;
+      c.bucket_end = 0xFFFFFFFFu;
+      c.use_tour = 0;
+    }
+    // an unbounded query whose groups are all cached: its distances are gathered
+    // from the cache (exact everywhere), and it starts at the bounds pass
+    GroupVecs gv{};
+    bool cached = !hop && !j->cache_dst;
+    for (int i = 0; i < q->k && cached; i++) cached = (gv.v[i] = grp->cache.vec(g->V, c.gid[i])) != nullptr;
+    if (cached) {
+      c.sssp_full = 1;
+      c.phase = PH_PREP;
+    }
+    c.sssp_mask = c.sssp_hops ? 2u : (c.bucket_end == 0xFFFFFFFFu ? 1u : 0u);
     cudaStream_t st = eng->stream;
     CK(cudaMemsetAsync(m.table, 0xFF, (size_t)g->V * (size_t)c.RW * 8, st));
     CK(cudaMemsetAsync(m.rowbits, 0, ((size_t)g->V + 31) / 32 * 4, st));
-    if (c.use_lb) CK(cudaMemsetAsync(m.dist, 0xFF, (size_t)g->V * DIST_STRIDE * 4, st));
+    if (c.use_lb && !cached) CK(cudaMemsetAsync(m.dist, 0xFF, (size_t)g->V * DIST_STRIDE * 4, st));
     if (c.sssp_mask) {
       CK(cudaMemsetAsync(m.fm[0], 0, ((size_t)g->V + 3) / 4 * 4, st));
       CK(cudaMemsetAsync(m.fm[1], 0, ((size_t)g->V + 3) / 4 * 4, st));
@@ -556,8 +589,18 @@ struct Runner {
     CK(cudaMemcpyAsync(d_ctx + s, &c, sizeof(Ctx), cudaMemcpyHostToDevice, st));
     cs.h2d += sizeof(Ctx) + sizeof(int32_t) * q->k;
     const DevGraph G = dev_graph(g);
+    if (cached) {
+      k_gather_dist<<<eng->sssp_blocks, 256, 0, st>>>(d_ctx + s, gv, g->V);
+      cs.launches += 1;
+    }
     k_init<<<dim3(64, 1), 256, 0, st>>>(d_ctx + s, 1, G, grp->d_ptr, grp->d_mem,
                                        eng->cfg.split_degree);
+    if (cached) {
+      // the bounds pass over the distance rows (star bound, group distances), which
+      // the control step after it turns into the tour table
+      k_sssp<<<eng->sssp_blocks, 256, 0, st>>>(d_ctx + s, 1, G, eng->cfg.split_degree);
+      cs.launches += 1;
+    }
     k_ctrl<<<1, 32, 0, st>>>(d_ctx + s, 1, CTRL_SSSP);
     cs.launches += 2;
     owner[s] = j;
@@ -753,6 +796,18 @@ struct Runner {
           !cap_is_worst(g->V, g->E, j->rw, eng->cfg.split_degree, c.qcap)) {
         j->boost++;
         retry.push_back(j);
+        continue;
+      }
+      if (j->cache_dst) {
+        // a group-cache fill: column 0 of the distance rows is the group's vector
+        if (!c.error && c.phase == PH_DONE)
+          CK(cudaMemcpy2DAsync(j->cache_dst, sizeof(uint32_t), mem[s].dist,
+                               DIST_STRIDE * sizeof(uint32_t), sizeof(uint32_t), (size_t)g->V,
+                               cudaMemcpyDeviceToDevice, eng->stream));
+        memset(j->out, 0, sizeof(gst_result));
+        j->out->status = c.error ? status_of(c) : GST_OK;
+        j->done = true;
+        done.push_back(j);
         continue;
       }
       const uint32_t nout = std::min(c.n_out, mem[s].outcap);
@@ -1200,48 +1255,17 @@ gst_status gst_groups_destroy(gst_groups* gr) {
   cudaStreamSynchronize(eng->stream);
   cudaFree(gr->d_ptr);
   cudaFree(gr->d_mem);
+  if (gr->cache.d_vec) cudaFree(gr->cache.d_vec);
   delete gr;
   return GST_OK;
 }
 
-gst_status gst_solve_batch(gst_graph* g, gst_groups* grp, int32_t n, const gst_query* queries,
-                           gst_result* results) {
-  gst_engine* eng = g ? g->eng : nullptr;
-  if (!g || !grp || grp->g != g || n < 0 || (n > 0 && (!queries || !results)))
-    return fail(eng, GST_BAD_INPUT, "solve: bad arguments");
-  for (int32_t i = 0; i < n; i++) memset(&results[i], 0, sizeof(gst_result));
-  std::lock_guard<std::mutex> lk(eng->mu);
-  CK(cudaSetDevice(eng->device));
-  const int B = std::max(1, std::min<int>(eng->cfg.max_batch, std::max<int32_t>(n, 1)));
-  if (!g->batch || g->batch->max_slots < B) {
-    g->batch.reset(new Runner(eng, g, std::max(B, g->batch ? g->batch->max_slots : 0)));
-    gst_status s = g->batch->init();
-    if (s != GST_OK) {
-      g->batch.reset();
-      return s;
-    }
-  }
-  Runner& R = *g->batch;
-  R.grp = grp;
-  R.cs = CallStats();
-  R.nctx = 0;  // no query is resident between calls
-  std::unique_ptr<Job[]> jobs(new Job[(size_t)std::max<int32_t>(n, 1)]);
-  std::deque<Job*> pending;
-  for (int32_t i = 0; i < n; i++) {
-    gst_status s = validate_query(eng, grp, &queries[i]);
-    if (s != GST_OK) {
-      results[i].status = s;
-      results[i].user_tag = queries[i].user_tag;
-      continue;
-    }
-    make_job(jobs[i], &queries[i], &results[i]);
-    pending.push_back(&jobs[i]);
-  }
-  cudaEvent_t ev0, ev1;
-  CK(cudaEventCreate(&ev0));
-  CK(cudaEventCreate(&ev1));
-  CK(cudaEventRecord(ev0, eng->stream));
-  // use at most B slots: admitting beyond max_batch would change the batch size
+namespace {
+// Run the pending jobs on R with at most B resident (admitting beyond the batch size
+// would change it), refilling slots as queries finish; capacity overflows are re-run
+// with more room.
+gst_status drive(Runner& R, std::deque<Job*>& pending, int B) {
+  gst_engine* eng = R.eng;
   const int saved = R.max_slots;
   R.max_slots = B;
   gst_status st = GST_OK;
@@ -1269,6 +1293,152 @@ gst_status gst_solve_batch(gst_graph* g, gst_groups* grp, int32_t n, const gst_q
     for (Job* j : retry) pending.push_front(j);
   }
   R.max_slots = saved;
+  return st;
+}
+
+// The graph's batch runner with at least B slots, created on first use.
+gst_status batch_runner(gst_graph* g, int B) {
+  if (!g->batch || g->batch->max_slots < B) {
+    const int slots = std::max(B, g->batch ? g->batch->max_slots : 0);
+    g->batch.reset(new Runner(g->eng, g, slots));
+    gst_status s = g->batch->init();
+    if (s != GST_OK) {
+      g->batch.reset();
+      return s;
+    }
+  }
+  return GST_OK;
+}
+}  // namespace
+
+gst_status gst_groups_cache_warm(gst_groups* grp, int32_t n, const int32_t* group_ids,
+                                 int64_t max_bytes, int32_t* n_cached) {
+  gst_engine* eng = grp ? grp->g->eng : nullptr;
+  if (!grp || n < 0 || (n > 0 && !group_ids) || max_bytes < 0)
+    return fail(eng, GST_BAD_INPUT, "cache: bad arguments");
+  for (int32_t i = 0; i < n; i++)
+    if (group_ids[i] < 0 || group_ids[i] >= grp->n) return fail(eng, GST_BAD_INPUT, "cache: group id out of range");
+  gst_graph* g = grp->g;
+  std::lock_guard<std::mutex> lk(eng->mu);
+  CK(cudaSetDevice(eng->device));
+  auto& C = grp->cache;
+  const size_t vb = (size_t)g->V * sizeof(uint32_t);
+  const int32_t cap = (int32_t)std::min<int64_t>(max_bytes / (int64_t)vb, grp->n);
+  if (cap != C.cap) {
+    CK(cudaStreamSynchronize(eng->stream));
+    if (C.d_vec) cudaFree(C.d_vec);
+    C = gst_groups::Cache();
+    if (cap > 0) {
+      CK(cudaMalloc(&C.d_vec, (size_t)cap * vb));
+      C.cap = cap;
+      C.slot_of.assign(grp->n, -1);
+      C.gid_of.assign(cap, -1);
+      C.used.assign(cap, 0);
+    }
+  }
+  if (n_cached) *n_cached = 0;
+  if (C.cap == 0) return GST_OK;
+  C.clock++;
+  // the listed groups, newest use first; at most cap of them stay
+  std::vector<int32_t> want;
+  for (int32_t i = 0; i < n && (int32_t)want.size() < C.cap; i++)
+    if (std::find(want.begin(), want.end(), group_ids[i]) == want.end()) want.push_back(group_ids[i]);
+  for (int32_t gid : want)
+    if (C.slot_of[gid] >= 0) C.used[C.slot_of[gid]] = C.clock;
+  std::vector<int32_t> todo;
+  for (int32_t gid : want)
+    if (C.slot_of[gid] < 0) todo.push_back(gid);
+  if (!todo.empty()) {
+    // a slot for each missing group: empty ones first, then the least recently used
+    // among groups this call does not list
+    std::unique_ptr<Job[]> jobs(new Job[todo.size()]);
+    std::vector<gst_result> res(todo.size());
+    std::deque<Job*> pending;
+    for (size_t t = 0; t < todo.size(); t++) {
+      int32_t best = -1;
+      for (int32_t sl = 0; sl < C.cap; sl++)
+        if (C.used[sl] != C.clock && (best < 0 || C.used[sl] < C.used[best])) best = sl;
+      if (C.gid_of[best] >= 0) C.slot_of[C.gid_of[best]] = -1;
+      C.gid_of[best] = todo[t];
+      C.used[best] = C.clock;
+      gst_query q{};
+      q.k = 1;
+      q.group_ids = &todo[t];
+      q.hop_bound = -1;
+      make_job(jobs[t], &q, &res[t]);
+      jobs[t].cache_dst = C.d_vec + (size_t)best * (size_t)g->V;
+      pending.push_back(&jobs[t]);
+    }
+    const int B = std::max(1, std::min<int>(eng->cfg.max_batch, (int)todo.size()));
+    gst_status st = batch_runner(g, B);
+    if (st == GST_OK) {
+      Runner& R = *g->batch;
+      R.grp = grp;
+      R.cs = CallStats();
+      R.nctx = 0;
+      st = drive(R, pending, B);
+    }
+    CK(cudaStreamSynchronize(eng->stream));
+    bool ok = st == GST_OK;
+    for (size_t t = 0; t < todo.size(); t++) ok = ok && jobs[t].done && res[t].status == GST_OK;
+    if (!ok) {
+      // forget the slots this call was filling (their groups were never visible)
+      for (int32_t sl = 0; sl < C.cap; sl++)
+        if (C.gid_of[sl] >= 0 && std::find(todo.begin(), todo.end(), C.gid_of[sl]) != todo.end()) {
+          C.gid_of[sl] = -1;
+          C.used[sl] = 0;
+        }
+      if (st != GST_OK) {
+        // a device failure ends the call; the runner is rebuilt on the next call
+        g->batch.reset();
+        cudaGetLastError();
+      } else {
+        st = GST_DEVICE_ERROR;
+      }
+      return fail(eng, st, "cache: a group's distance search failed: " + eng->err);
+    }
+    for (int32_t sl = 0; sl < C.cap; sl++)
+      if (C.gid_of[sl] >= 0) C.slot_of[C.gid_of[sl]] = sl;
+  }
+  if (n_cached)
+    for (int32_t gid : want) *n_cached += C.slot_of[gid] >= 0;
+  return GST_OK;
+}
+
+gst_status gst_solve_batch(gst_graph* g, gst_groups* grp, int32_t n, const gst_query* queries,
+                           gst_result* results) {
+  gst_engine* eng = g ? g->eng : nullptr;
+  if (!g || !grp || grp->g != g || n < 0 || (n > 0 && (!queries || !results)))
+    return fail(eng, GST_BAD_INPUT, "solve: bad arguments");
+  for (int32_t i = 0; i < n; i++) memset(&results[i], 0, sizeof(gst_result));
+  std::lock_guard<std::mutex> lk(eng->mu);
+  CK(cudaSetDevice(eng->device));
+  const int B = std::max(1, std::min<int>(eng->cfg.max_batch, std::max<int32_t>(n, 1)));
+  {
+    gst_status s = batch_runner(g, B);
+    if (s != GST_OK) return s;
+  }
+  Runner& R = *g->batch;
+  R.grp = grp;
+  R.cs = CallStats();
+  R.nctx = 0;  // no query is resident between calls
+  std::unique_ptr<Job[]> jobs(new Job[(size_t)std::max<int32_t>(n, 1)]);
+  std::deque<Job*> pending;
+  for (int32_t i = 0; i < n; i++) {
+    gst_status s = validate_query(eng, grp, &queries[i]);
+    if (s != GST_OK) {
+      results[i].status = s;
+      results[i].user_tag = queries[i].user_tag;
+      continue;
+    }
+    make_job(jobs[i], &queries[i], &results[i]);
+    pending.push_back(&jobs[i]);
+  }
+  cudaEvent_t ev0, ev1;
+  CK(cudaEventCreate(&ev0));
+  CK(cudaEventCreate(&ev1));
+  CK(cudaEventRecord(ev0, eng->stream));
+  gst_status st = drive(R, pending, B);
   CK(cudaEventRecord(ev1, eng->stream));
   CK(cudaEventSynchronize(ev1));
   float ms = 0;

@@ -327,6 +327,7 @@ C_ABI_SYMBOLS = [
     "gst_groups_destroy", "gst_solve", "gst_solve_batch", "gst_result_free",
     "gst_server_create", "gst_submit", "gst_poll", "gst_wait", "gst_server_destroy",
     "gst_debug_slot_state", "gst_solve_noalloc", "gst_engine_set_profiling", "gst_autotune",
+    "gst_groups_cache_warm",
 ]
 
 
@@ -420,6 +421,17 @@ class DeviceGraph:
                                     C.byref(self._grp))
         if rc:
             raise GstError(f"gst_groups_create: {STATUS.get(rc, rc)}: {eng.error()}")
+
+    def cache_warm(self, group_ids, max_bytes: int) -> int:
+        """Keep the one-label distances of these groups on the device (include/gst.h:
+        gst_groups_cache_warm); returns how many of them are cached."""
+        a = np.ascontiguousarray(group_ids, dtype=np.int32)
+        n = C.c_int32(0)
+        rc = _lib.gst_groups_cache_warm(self._grp, len(a), a.ctypes.data_as(C.POINTER(C.c_int32)),
+                                        C.c_int64(max_bytes), C.byref(n))
+        if rc:
+            raise GstError(f"gst_groups_cache_warm: {STATUS.get(rc, rc)}: {self.eng.error()}")
+        return n.value
 
     def close(self):
         if self._grp:

@@ -142,6 +142,18 @@ gst_status gst_groups_create(gst_graph* g, int32_t n_groups, const int64_t* grp_
                              const int32_t* members, gst_groups** out);
 gst_status gst_groups_destroy(gst_groups* grp);
 
+/* One-label distance cache for serving hot groups (no counterpart in the reference,
+ * which recomputes a group's distances for every query: mapper_enactor.cuh:249-366).
+ * A group's distances to every vertex depend on the group only.  This computes them,
+ * without cutoff, for each listed group not yet cached and keeps them on the device,
+ * up to max_bytes (4 x V bytes per group; when the list holds more groups than fit,
+ * the first ones are kept; groups of earlier calls that this call does not list are
+ * replaced least recently used first).  Unbounded queries whose groups are all cached
+ * then skip the distance search.  A different max_bytes drops the cache first;
+ * max_bytes = 0 frees it.  *n_cached (optional) = listed groups now cached. */
+gst_status gst_groups_cache_warm(gst_groups* grp, int32_t n, const int32_t* group_ids,
+                                 int64_t max_bytes, int32_t* n_cached);
+
 /* One query, synchronous.  Fills *res (call gst_result_free afterwards). */
 gst_status gst_solve(gst_graph* g, gst_groups* grp, const gst_query* q, gst_result* res);
 
