@@ -1,7 +1,7 @@
 """Benchmark: exact-cost GST queries/s on the mid-scale power-law workload.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload c2|c1] [--batch B]
+                    [--workload c2|c1|c4|c5] [--batch B]
 
 Workload (default "c2", the reference's plain single-query GPU configuration at
 mid scale): R-MAT (a,b,c) = (0.57, 0.19, 0.19), V = 170,000 target, 6.8M
@@ -63,6 +63,12 @@ WORKLOADS = {
                groups=("zipf", 20_000, 1.5, 2, 2000, SEED + 1004),
                queries=[(3, 410, SEED + 2041), (5, 410, SEED + 2042), (7, 204, SEED + 2043)],
                hop=(4, 0.5, SEED + 3004)),
+    # serving form: k uniform in 3..8, 30 % with hop bound 4 (a k = 8, D = 4 state table,
+    # 16M x 256 x 5 cells x 8 B = 172 GB, exceeds one GPU: those draws stay unbounded)
+    "c5": dict(name="rmat16M_250M_k3to8_30pctD", graph=("rmat", 16_000_000, 250_000_000, SEED + 5),
+               groups=("zipf", 50_000, 1.5, 2, 5000, SEED + 1005),
+               queries=[(k, 100, SEED + 2050 + k) for k in range(3, 9)],
+               hop=(4, 0.3, SEED + 3005), hop_kmax=7),
 }
 
 
@@ -90,6 +96,8 @@ def make_workload(key):
         order = rng.permutation(len(allq))
         queries = [allq[i] for i in order]
         hops = [D if x < frac else None for x in rng.random(len(queries))]
+        kmax = w.get("hop_kmax", 8)
+        hops = [h if len(q) <= kmax else None for q, h in zip(queries, hops)]
         return w, g, grp, queries, hops
     # interleave the k classes: k5, k7, k5, k7, ...
     for i in range(max(len(p) for p in pools)):
