@@ -353,8 +353,14 @@ struct Runner {
     idle_written.assign(max_slots, 0);
     size_t free_b = 0, total_b = 0;
     CK(cudaMemGetInfo(&free_b, &total_b));
+    // memory the engine's pool keeps but no allocation uses (arenas released by another
+    // runner) is free for this one's slots too
+    unsigned long long reserved = 0, used = 0;
+    CK(cudaMemPoolGetAttribute(eng->pool, cudaMemPoolAttrReservedMemCurrent, &reserved));
+    CK(cudaMemPoolGetAttribute(eng->pool, cudaMemPoolAttrUsedMemCurrent, &used));
+    const size_t avail = free_b + (size_t)(reserved > used ? reserved - used : 0);
     budget = eng->cfg.mem_budget_bytes > 0 ? (size_t)eng->cfg.mem_budget_bytes
-                                           : (size_t)(free_b * 0.85);
+                                           : (size_t)(avail * 0.85);
     return GST_OK;
   }
 
@@ -1701,6 +1707,9 @@ gst_status gst_server_create(gst_graph* g, gst_groups* grp, gst_server** out) {
   {
     std::lock_guard<std::mutex> lk(eng->mu);
     CK(cudaSetDevice(eng->device));
+    // the graph's batch runner holds no query between calls: hand its slot memory to
+    // the server (the next gst_solve* call makes a new one from what is free then)
+    g->batch.reset();
     sv->run.reset(new Runner(eng, g, std::max(1, eng->cfg.max_batch)));
     sv->run->grp = grp;
     gst_status s = sv->run->init();
