@@ -1269,7 +1269,8 @@ gst_status gst_groups_destroy(gst_groups* gr) {
 namespace {
 // Run the pending jobs on R with at most B resident (admitting beyond the batch size
 // would change it), refilling slots as queries finish; capacity overflows are re-run
-// with more room.
+// with more room.  A job that does not fit the free memory yet does not hold back the
+// smaller ones behind it (a batch has no arrival order to keep).
 gst_status drive(Runner& R, std::deque<Job*>& pending, int B) {
   gst_engine* eng = R.eng;
   const int saved = R.max_slots;
@@ -1277,11 +1278,14 @@ gst_status drive(Runner& R, std::deque<Job*>& pending, int B) {
   gst_status st = GST_OK;
   std::vector<Job*> done, retry;
   while (st == GST_OK && (!pending.empty() || R.active > 0)) {
-    while (!pending.empty()) {
-      gst_status s = R.admit(pending.front());
-      if (s == GST_NOT_READY) break;
+    for (auto it = pending.begin(); it != pending.end() && R.active < R.max_slots;) {
+      gst_status s = R.admit(*it);
+      if (s == GST_NOT_READY) {
+        ++it;
+        continue;
+      }
       if (s == GST_OOM_ADMISSION) {
-        Job* j = pending.front();
+        Job* j = *it;
         j->out->status = GST_OOM_ADMISSION;
         j->out->user_tag = j->q.user_tag;
         fail(eng, GST_OOM_ADMISSION, "solve: the query's state table does not fit the memory budget");
@@ -1289,7 +1293,7 @@ gst_status drive(Runner& R, std::deque<Job*>& pending, int B) {
         st = s;
         break;
       }
-      pending.pop_front();
+      it = pending.erase(it);
     }
     if (st != GST_OK || R.active == 0) break;
     st = R.run(0);
