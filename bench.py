@@ -292,7 +292,10 @@ def run_reference_arm(args):
         "warmup": args.warmup, "ms_per_step": 1e3 * spent / max(1, args.steps),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic", "impl": "reference",
-        "config": {"workload": w["name"], "parallelism": "cpu"},
+        "config": {"workload": w["name"], "V": g.V, "E_directed": g.E,
+                   "global_batch": args.batch * n, "k": sorted({len(q) for q in queries}),
+                   "hop_bounded": sum(h is not None for h in hops) / len(hops),
+                   "parallelism": "cpu", "autotuned": None, "l2": "not applicable (host cores)"},
         "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": threads,
                          "kind": "reference", "sample": sample},
         "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0,
