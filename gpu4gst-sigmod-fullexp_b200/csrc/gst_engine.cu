@@ -417,11 +417,13 @@ struct Runner {
       return;
     }
   }
-  // Reserve a new arena of at least `need` bytes (4 GB chunks) within the budget.
+  // Reserve a new arena of at least `need` bytes within the budget: at least 4 GB, and
+  // at least what is held already (geometric growth: mixed batches stop growing the
+  // arenas after their first few, since new physical memory costs ~8-9 ms per GB).
   gst_status arena_grow(size_t need, bool* grown) {
     *grown = false;
     if (held + need > budget) return GST_OK;
-    const size_t chunk = std::max(need, std::min((size_t)4 << 30, budget - held));
+    const size_t chunk = std::max(need, std::min(std::max((size_t)4 << 30, held), budget - held));
     void* p = nullptr;
     const auto ta = Clock::now();
     CK(cudaMallocFromPoolAsync(&p, chunk, eng->pool, eng->stream));
