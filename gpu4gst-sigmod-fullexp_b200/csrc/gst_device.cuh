@@ -30,11 +30,16 @@
 //   control       one thread per query swaps worklists, advances the cost bucket
 //                 (near/far ordering), counts levels and detects the fixpoint
 //                 (replaces the grid barrier loop of mapper_enactor.cuh:158-246).
-// Pruning (all safe with ub >= optimum; see the engine's design notes):
+// Pruning (every test compares with ub, the cost of a feasible tree, so no state of
+// an optimal tree is dropped):
 //   grow a state only if 2c <= ub (code/TrimCDP-WB/include/mapper_enactor.cuh /
 //   reducer.cuh:317-433 use c-1 <= best/2); keep a merged non-full state only if
 //   3c <= 2ub (PrunedDP++ CPUNONHOP.h:913 uses 0.667*best+2); drop a state if
-//   c + max_{i not in X} dist_i(v) > ub (one-label bound, get_lb mapper.cuh:163-191).
+//   c + max_{i not in X} dist_i(v) > ub (one-label bound, get_lb mapper.cuh:163-191)
+//   or c + ceil(tour/2) > ub (tour bound, PrunedDP++ CPUNONHOP.h:433-493).  A
+//   hop-bounded state of height d takes its distances within the hop budget D - d
+//   (its deepest vertex is d edges below v, so every missing group lies within
+//   D - d edges of v in any tree of diameter <= D that contains it).
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -63,7 +68,7 @@ enum CtrlMode : int { CTRL_SSSP = 0, CTRL_DP_ROWS = 1, CTRL_DP_GROW = 2 };
 // needs, over-counting by at most a third.
 constexpr int WIDX = 16;
 constexpr uint32_t CHUNK = 0x80000000u;  // item flag (in pd): one `split`-edge chunk only
-constexpr int RELAX_U = 4;               // edges per lane per round of the relax loops
+constexpr int RELAX_U = 4;               // edges per lane per round of the grow relax loop
 // Hop-limited distance items carry their path's edge count in bits 8..15 of the
 // group word (group index in bits 0..7).
 constexpr uint32_t SSSP_HOP_SHIFT = 8;
@@ -209,21 +214,9 @@ __device__ __forceinline__ uint64_t pack_cell(uint32_t cost, uint32_t low) {
   return ((uint64_t)cost << 32) | low;
 }
 
-// b-th (1-based) non-empty submask of `mask`, bits of b deposited into mask's bits.
-__device__ __forceinline__ uint32_t deposit(uint32_t b, uint32_t mask) {
-  uint32_t r = 0;
-  while (mask) {
-    const uint32_t low = mask & (0u - mask);
-    if (b & 1u) r |= low;
-    b >>= 1;
-    mask ^= low;
-  }
-  return r;
-}
-
-// Submask table for masks of up to 8 bits: SUBMASK.v[M][b] = deposit(b, M) (the bits
-// of b placed into the set bits of M, lowest first), built at compile time, so that
-// the merge loop enumerates the submasks of a complement with one cached load.
+// Submask table for masks of up to 8 bits: SUBMASK.v[M][b] is the b-th submask of M,
+// the bits of b placed into the set bits of M, lowest first.  Built at compile time,
+// so that the merge loop enumerates the submasks of a complement with one cached load.
 struct SubmaskTable {
   unsigned char v[256][256];
 };
