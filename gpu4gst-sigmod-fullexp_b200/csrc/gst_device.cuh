@@ -519,7 +519,8 @@ __device__ __forceinline__ void add_stat(Ctx* ctxs, int qi, bool valid, uint32_t
 
 // ---- group cache: distance rows of a query from cached per-group vectors ----------
 struct GroupVecs {
-  const uint32_t* v[KMAX];  // d_i(.) of the query's i-th group, V entries each
+  const uint32_t* v[KMAX];  // d_i(.) of the query's i-th group, V entries each (nullptr:
+                            // not cached, left unreached for the distance search)
 };
 __global__ void k_gather_dist(Ctx* c, GroupVecs gv, int64_t V) {
   const int k = c->k;
@@ -527,7 +528,7 @@ __global__ void k_gather_dist(Ctx* c, GroupVecs gv, int64_t V) {
        v += (int64_t)gridDim.x * blockDim.x) {
     uint32_t d[KMAX];
 #pragma unroll
-    for (int i = 0; i < KMAX; i++) d[i] = i < k ? __ldg(&gv.v[i][v]) : COST_INF;
+    for (int i = 0; i < KMAX; i++) d[i] = i < k && gv.v[i] ? __ldg(&gv.v[i][v]) : COST_INF;
     uint4* row = (uint4*)&c->dist[(uint64_t)v * DIST_STRIDE];
     row[0] = make_uint4(d[0], d[1], d[2], d[3]);
     row[1] = make_uint4(d[4], d[5], d[6], d[7]);

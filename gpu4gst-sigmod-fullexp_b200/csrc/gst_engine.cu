@@ -574,12 +574,16 @@ struct Runner {
       c.bucket_end = 0xFFFFFFFFu;
       c.use_tour = 0;
     }
-    // an unbounded query whose groups are all cached: its distances are gathered
-    // from the cache (exact everywhere), and it starts at the bounds pass
+    // an unbounded query with cached groups: their distances are gathered from the
+    // cache (exact everywhere; a member's distance 0 keeps its group out of the search).
+    // With every group cached the query starts at the bounds pass; otherwise the search
+    // runs for the other groups, its star bound already counting the cached ones.
     GroupVecs gv{};
-    bool cached = !hop && !j->cache_dst;
-    for (int i = 0; i < q->k && cached; i++) cached = (gv.v[i] = grp->cache.vec(g->V, c.gid[i])) != nullptr;
-    if (cached) {
+    int n_cached = 0;
+    if (!hop && !j->cache_dst)
+      for (int i = 0; i < q->k; i++) n_cached += (gv.v[i] = grp->cache.vec(g->V, c.gid[i])) != nullptr;
+    const bool cached = n_cached > 0;
+    if (n_cached == q->k) {
       c.sssp_full = 1;
       c.phase = PH_PREP;
     }
@@ -603,7 +607,7 @@ struct Runner {
     }
     k_init<<<dim3(64, 1), 256, 0, st>>>(d_ctx + s, 1, G, grp->d_ptr, grp->d_mem,
                                        eng->cfg.split_degree);
-    if (cached) {
+    if (n_cached == q->k) {
       // the bounds pass over the distance rows (star bound, group distances), which
       // the control step after it turns into the tour table
       k_sssp<<<eng->sssp_blocks, 256, 0, st>>>(d_ctx + s, 1, G, eng->cfg.split_degree);

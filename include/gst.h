@@ -149,7 +149,8 @@ gst_status gst_groups_destroy(gst_groups* grp);
  * up to max_bytes (4 x V bytes per group; when the list holds more groups than fit,
  * the first ones are kept; groups of earlier calls that this call does not list are
  * replaced least recently used first).  Unbounded queries whose groups are all cached
- * then skip the distance search.  A different max_bytes drops the cache first;
+ * then skip the distance search; with some of their groups cached, the search runs for
+ * the others only.  A different max_bytes drops the cache first;
  * max_bytes = 0 frees it.  *n_cached (optional) = listed groups now cached. */
 gst_status gst_groups_cache_warm(gst_groups* grp, int32_t n, const int32_t* group_ids,
                                  int64_t max_bytes, int32_t* n_cached);
