@@ -522,14 +522,14 @@ struct GroupVecs {
   const uint32_t* v[KMAX];  // d_i(.) of the query's i-th group, V entries each (nullptr:
                             // not cached, left unreached for the distance search)
 };
-__global__ void k_gather_dist(Ctx* c, GroupVecs gv, int64_t V) {
-  const int k = c->k;
+// rows: V x DIST_STRIDE distance rows (the distance table, or one hop budget's table)
+__global__ void k_gather_dist(uint32_t* rows, int k, GroupVecs gv, int64_t V) {
   for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < V;
        v += (int64_t)gridDim.x * blockDim.x) {
     uint32_t d[KMAX];
 #pragma unroll
     for (int i = 0; i < KMAX; i++) d[i] = i < k && gv.v[i] ? __ldg(&gv.v[i][v]) : COST_INF;
-    uint4* row = (uint4*)&c->dist[(uint64_t)v * DIST_STRIDE];
+    uint4* row = (uint4*)&rows[(uint64_t)v * DIST_STRIDE];
     row[0] = make_uint4(d[0], d[1], d[2], d[3]);
     row[1] = make_uint4(d[4], d[5], d[6], d[7]);
   }

@@ -164,21 +164,25 @@ struct gst_groups {
   int64_t* d_ptr = nullptr;
   int32_t* d_mem = nullptr;
   std::vector<int64_t> h_ptr;
-  // One-label distance cache: the distances of a group to every vertex depend on the
-  // group only, not on the query, so hot groups keep theirs on the device (V uint32
-  // per cached group, least recently warmed replaced first).
+  // One-label distance caches: the distances of a group to every vertex depend on the
+  // group only, not on the query, so hot groups keep theirs on the device (least
+  // recently warmed replaced first).  `cache`: unlimited distances, V uint32 per group.
+  // `hop_cache`: the distances within hop budgets 1..n (n = min(D-1, 7)) and within D
+  // for one hop bound D, (n+1) x V uint32 per group in that order.
   struct Cache {
-    uint32_t* d_vec = nullptr;       // cap x V
+    uint32_t* d_vec = nullptr;       // cap x stride
     int32_t cap = 0;
+    int32_t D = -1;                  // hop bound of the entries (-1: unlimited)
+    size_t stride = 0;               // uint32 per entry
     std::vector<int32_t> slot_of;    // group id -> slot, -1 if not cached
     std::vector<int32_t> gid_of;     // slot -> group id, -1 if empty
     std::vector<uint64_t> used;      // slot -> last warm call that listed it
     uint64_t clock = 0;
-    const uint32_t* vec(int64_t V, int32_t gid) const {
+    const uint32_t* vec(int32_t gid) const {
       const int32_t s = gid >= 0 && gid < (int32_t)slot_of.size() ? slot_of[gid] : -1;
-      return s < 0 ? nullptr : d_vec + (size_t)s * (size_t)V;
+      return s < 0 ? nullptr : d_vec + (size_t)s * stride;
     }
-  } cache;
+  } cache, hop_cache;
 };
 
 namespace {
@@ -574,14 +578,24 @@ struct Runner {
       c.bucket_end = 0xFFFFFFFFu;
       c.use_tour = 0;
     }
-    // an unbounded query with cached groups: their distances are gathered from the
+    // An unbounded query with cached groups: their distances are gathered from the
     // cache (exact everywhere; a member's distance 0 keeps its group out of the search).
     // With every group cached the query starts at the bounds pass; otherwise the search
-    // runs for the other groups, its star bound already counting the cached ones.
+    // runs for the other groups, its star bound already counting the cached ones.  A
+    // hop-bounded query uses the hop cache only when all its groups are cached for its
+    // bound: then every hop budget's table is gathered too.
     GroupVecs gv{};
+    const uint32_t* hv[KMAX] = {};
     int n_cached = 0;
-    if (!hop && !j->cache_dst)
-      for (int i = 0; i < q->k; i++) n_cached += (gv.v[i] = grp->cache.vec(g->V, c.gid[i])) != nullptr;
+    const size_t V = (size_t)g->V;
+    if (!hop && !j->cache_dst) {
+      for (int i = 0; i < q->k; i++) n_cached += (gv.v[i] = grp->cache.vec(c.gid[i])) != nullptr;
+    } else if (hop && q->hop_bound > 0 && !j->cache_dst && grp->hop_cache.cap > 0 &&
+               grp->hop_cache.D == q->hop_bound) {
+      for (int i = 0; i < q->k; i++) n_cached += (hv[i] = grp->hop_cache.vec(c.gid[i])) != nullptr;
+      if (n_cached < q->k) n_cached = 0;
+      for (int i = 0; i < q->k && n_cached; i++) gv.v[i] = hv[i] + (size_t)c.nhb * V;
+    }
     const bool cached = n_cached > 0;
     if (n_cached == q->k) {
       c.sssp_full = 1;
@@ -596,14 +610,22 @@ struct Runner {
       CK(cudaMemsetAsync(m.fm[0], 0, ((size_t)g->V + 3) / 4 * 4, st));
       CK(cudaMemsetAsync(m.fm[1], 0, ((size_t)g->V + 3) / 4 * 4, st));
     }
-    if (c.nhb)
+    if (c.nhb && !cached)
       CK(cudaMemsetAsync(m.dist_h, 0xFF, (size_t)c.nhb * (size_t)g->V * DIST_STRIDE * 4, st));
     CK(cudaMemcpyAsync(d_ctx + s, &c, sizeof(Ctx), cudaMemcpyHostToDevice, st));
     cs.h2d += sizeof(Ctx) + sizeof(int32_t) * q->k;
     const DevGraph G = dev_graph(g);
     if (cached) {
-      k_gather_dist<<<eng->sssp_blocks, 256, 0, st>>>(d_ctx + s, gv, g->V);
+      k_gather_dist<<<eng->sssp_blocks, 256, 0, st>>>(m.dist, q->k, gv, g->V);
       cs.launches += 1;
+      if (hop)
+        for (int h = 1; h <= c.nhb; h++) {
+          GroupVecs gh{};
+          for (int i = 0; i < q->k; i++) gh.v[i] = hv[i] + (size_t)(h - 1) * V;
+          k_gather_dist<<<eng->sssp_blocks, 256, 0, st>>>(
+              m.dist_h + (size_t)(h - 1) * V * DIST_STRIDE, q->k, gh, g->V);
+          cs.launches += 1;
+        }
     }
     k_init<<<dim3(64, 1), 256, 0, st>>>(d_ctx + s, 1, G, grp->d_ptr, grp->d_mem,
                                        eng->cfg.split_degree);
@@ -811,11 +833,19 @@ struct Runner {
         continue;
       }
       if (j->cache_dst) {
-        // a group-cache fill: column 0 of the distance rows is the group's vector
-        if (!c.error && c.phase == PH_DONE)
-          CK(cudaMemcpy2DAsync(j->cache_dst, sizeof(uint32_t), mem[s].dist,
-                               DIST_STRIDE * sizeof(uint32_t), sizeof(uint32_t), (size_t)g->V,
+        // a group-cache fill: column 0 of the distance rows is the group's vector; a hop
+        // fill stores its budgets 1..nhb first, then the full bound
+        if (!c.error && c.phase == PH_DONE) {
+          const size_t V = (size_t)g->V;
+          CK(cudaMemcpy2DAsync(j->cache_dst + (size_t)c.nhb * V, sizeof(uint32_t), mem[s].dist,
+                               DIST_STRIDE * sizeof(uint32_t), sizeof(uint32_t), V,
                                cudaMemcpyDeviceToDevice, eng->stream));
+          for (int h = 1; h <= c.nhb; h++)
+            CK(cudaMemcpy2DAsync(j->cache_dst + (size_t)(h - 1) * V, sizeof(uint32_t),
+                                 mem[s].dist_h + (size_t)(h - 1) * V * DIST_STRIDE,
+                                 DIST_STRIDE * sizeof(uint32_t), sizeof(uint32_t), V,
+                                 cudaMemcpyDeviceToDevice, eng->stream));
+        }
         memset(j->out, 0, sizeof(gst_result));
         j->out->status = c.error ? status_of(c) : GST_OK;
         j->done = true;
@@ -1268,6 +1298,7 @@ gst_status gst_groups_destroy(gst_groups* gr) {
   cudaFree(gr->d_ptr);
   cudaFree(gr->d_mem);
   if (gr->cache.d_vec) cudaFree(gr->cache.d_vec);
+  if (gr->hop_cache.d_vec) cudaFree(gr->hop_cache.d_vec);
   delete gr;
   return GST_OK;
 }
@@ -1327,26 +1358,25 @@ gst_status batch_runner(gst_graph* g, int B) {
 }
 }  // namespace
 
-gst_status gst_groups_cache_warm(gst_groups* grp, int32_t n, const int32_t* group_ids,
-                                 int64_t max_bytes, int32_t* n_cached) {
-  gst_engine* eng = grp ? grp->g->eng : nullptr;
-  if (!grp || n < 0 || (n > 0 && !group_ids) || max_bytes < 0)
-    return fail(eng, GST_BAD_INPUT, "cache: bad arguments");
-  for (int32_t i = 0; i < n; i++)
-    if (group_ids[i] < 0 || group_ids[i] >= grp->n) return fail(eng, GST_BAD_INPUT, "cache: group id out of range");
+namespace {
+// Warm cache C of groups grp for hop bound D (-1: unlimited distances): see
+// gst_groups_cache_warm / gst_groups_cache_warm_hop.  Caller holds the engine lock.
+gst_status cache_warm(gst_groups* grp, gst_groups::Cache& C, int32_t D, int32_t n,
+                      const int32_t* group_ids, int64_t max_bytes, int32_t* n_cached) {
   gst_graph* g = grp->g;
-  std::lock_guard<std::mutex> lk(eng->mu);
-  CK(cudaSetDevice(eng->device));
-  auto& C = grp->cache;
-  const size_t vb = (size_t)g->V * sizeof(uint32_t);
-  const int32_t cap = (int32_t)std::min<int64_t>(max_bytes / (int64_t)vb, grp->n);
-  if (cap != C.cap) {
+  gst_engine* eng = g->eng;
+  const size_t stride = (size_t)g->V * (size_t)(D > 0 ? hop_budgets(D) + 1 : 1);
+  const size_t eb = stride * sizeof(uint32_t);
+  const int32_t cap = (int32_t)std::min<int64_t>(max_bytes / (int64_t)eb, grp->n);
+  if (cap != C.cap || D != C.D) {
     CK(cudaStreamSynchronize(eng->stream));
     if (C.d_vec) cudaFree(C.d_vec);
     C = gst_groups::Cache();
     if (cap > 0) {
-      CK(cudaMalloc(&C.d_vec, (size_t)cap * vb));
+      CK(cudaMalloc(&C.d_vec, (size_t)cap * eb));
       C.cap = cap;
+      C.D = D;
+      C.stride = stride;
       C.slot_of.assign(grp->n, -1);
       C.gid_of.assign(cap, -1);
       C.used.assign(cap, 0);
@@ -1355,7 +1385,7 @@ gst_status gst_groups_cache_warm(gst_groups* grp, int32_t n, const int32_t* grou
   if (n_cached) *n_cached = 0;
   if (C.cap == 0) return GST_OK;
   C.clock++;
-  // the listed groups, newest use first; at most cap of them stay
+  // the listed groups, in list order; at most cap of them stay
   std::vector<int32_t> want;
   for (int32_t i = 0; i < n && (int32_t)want.size() < C.cap; i++)
     if (std::find(want.begin(), want.end(), group_ids[i]) == want.end()) want.push_back(group_ids[i]);
@@ -1366,7 +1396,7 @@ gst_status gst_groups_cache_warm(gst_groups* grp, int32_t n, const int32_t* grou
     if (C.slot_of[gid] < 0) todo.push_back(gid);
   if (!todo.empty()) {
     // a slot for each missing group: empty ones first, then the least recently used
-    // among groups this call does not list
+    // among groups this call does not list; one distance-only job per group
     std::unique_ptr<Job[]> jobs(new Job[todo.size()]);
     std::vector<gst_result> res(todo.size());
     std::deque<Job*> pending;
@@ -1380,9 +1410,9 @@ gst_status gst_groups_cache_warm(gst_groups* grp, int32_t n, const int32_t* grou
       gst_query q{};
       q.k = 1;
       q.group_ids = &todo[t];
-      q.hop_bound = -1;
+      q.hop_bound = D;
       make_job(jobs[t], &q, &res[t]);
-      jobs[t].cache_dst = C.d_vec + (size_t)best * (size_t)g->V;
+      jobs[t].cache_dst = C.d_vec + (size_t)best * C.stride;
       pending.push_back(&jobs[t]);
     }
     const int B = std::max(1, std::min<int>(eng->cfg.max_batch, (int)todo.size()));
@@ -1419,6 +1449,31 @@ gst_status gst_groups_cache_warm(gst_groups* grp, int32_t n, const int32_t* grou
   if (n_cached)
     for (int32_t gid : want) *n_cached += C.slot_of[gid] >= 0;
   return GST_OK;
+}
+}  // namespace
+
+gst_status gst_groups_cache_warm(gst_groups* grp, int32_t n, const int32_t* group_ids,
+                                 int64_t max_bytes, int32_t* n_cached) {
+  gst_engine* eng = grp ? grp->g->eng : nullptr;
+  if (!grp || n < 0 || (n > 0 && !group_ids) || max_bytes < 0)
+    return fail(eng, GST_BAD_INPUT, "cache: bad arguments");
+  for (int32_t i = 0; i < n; i++)
+    if (group_ids[i] < 0 || group_ids[i] >= grp->n) return fail(eng, GST_BAD_INPUT, "cache: group id out of range");
+  std::lock_guard<std::mutex> lk(eng->mu);
+  CK(cudaSetDevice(eng->device));
+  return cache_warm(grp, grp->cache, -1, n, group_ids, max_bytes, n_cached);
+}
+
+gst_status gst_groups_cache_warm_hop(gst_groups* grp, int32_t n, const int32_t* group_ids,
+                                     int32_t hop_bound, int64_t max_bytes, int32_t* n_cached) {
+  gst_engine* eng = grp ? grp->g->eng : nullptr;
+  if (!grp || n < 0 || (n > 0 && !group_ids) || max_bytes < 0 || hop_bound < 1 || hop_bound > 30)
+    return fail(eng, GST_BAD_INPUT, "cache: bad arguments (hop bound must be in [1, 30])");
+  for (int32_t i = 0; i < n; i++)
+    if (group_ids[i] < 0 || group_ids[i] >= grp->n) return fail(eng, GST_BAD_INPUT, "cache: group id out of range");
+  std::lock_guard<std::mutex> lk(eng->mu);
+  CK(cudaSetDevice(eng->device));
+  return cache_warm(grp, grp->hop_cache, hop_bound, n, group_ids, max_bytes, n_cached);
 }
 
 gst_status gst_solve_batch(gst_graph* g, gst_groups* grp, int32_t n, const gst_query* queries,

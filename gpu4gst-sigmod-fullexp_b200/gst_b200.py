@@ -327,7 +327,7 @@ C_ABI_SYMBOLS = [
     "gst_groups_destroy", "gst_solve", "gst_solve_batch", "gst_result_free",
     "gst_server_create", "gst_submit", "gst_poll", "gst_wait", "gst_server_destroy",
     "gst_debug_slot_state", "gst_solve_noalloc", "gst_engine_set_profiling", "gst_autotune",
-    "gst_groups_cache_warm",
+    "gst_groups_cache_warm", "gst_groups_cache_warm_hop",
 ]
 
 
@@ -431,6 +431,19 @@ class DeviceGraph:
                                         C.c_int64(max_bytes), C.byref(n))
         if rc:
             raise GstError(f"gst_groups_cache_warm: {STATUS.get(rc, rc)}: {self.eng.error()}")
+        return n.value
+
+    def cache_warm_hop(self, group_ids, hop_bound: int, max_bytes: int) -> int:
+        """The same for hop-bounded queries with this bound (include/gst.h:
+        gst_groups_cache_warm_hop)."""
+        a = np.ascontiguousarray(group_ids, dtype=np.int32)
+        n = C.c_int32(0)
+        rc = _lib.gst_groups_cache_warm_hop(self._grp, len(a),
+                                            a.ctypes.data_as(C.POINTER(C.c_int32)),
+                                            C.c_int32(hop_bound), C.c_int64(max_bytes),
+                                            C.byref(n))
+        if rc:
+            raise GstError(f"gst_groups_cache_warm_hop: {STATUS.get(rc, rc)}: {self.eng.error()}")
         return n.value
 
     def close(self):

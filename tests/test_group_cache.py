@@ -103,3 +103,35 @@ def test_cache_replacement_and_partial_hits(engine):
         assert a.status == want.status and a.cost == want.cost
     finally:
         dg.close()
+
+
+def test_hop_cache_matches_reference(engine):
+    """Hop-bounded queries whose groups are all cached for their bound skip the distance
+    search (every hop budget's table gathered) and return the reference's costs; other
+    bounds, and queries with a group not cached, take the normal path."""
+    for name in ("rmat3k_k4_k5", "rmat50k_hop"):
+        fx = load_golden(name)
+        g, grp = golden_inputs(fx)
+        dg = engine.graph(g, grp)
+        try:
+            cases = [x for x in _cases(fx) if x[1] is not None and x[1] > 0]
+            for D in sorted({h for _, h, _ in cases}):
+                mine = [x for x in cases if x[1] == D][:10]
+                gids = sorted({x for q, _, _ in mine for x in q})
+                per = 4 * g.V * (min(D - 1, 7) + 1)
+                assert dg.cache_warm_hop(gids, D, per * len(gids)) == len(gids)
+                for q, h, c in mine:
+                    a = dg.solve(q, h)
+                    _check(g, grp, q, h, a, c)
+                    assert a.stats["sssp_relaxations"] == 0
+                qs = [q for q, _, _ in mine]
+                for (q, h, c), a in zip(mine, dg.solve_batch(qs, [D] * len(qs))):
+                    _check(g, grp, q, h, a, c)
+                # another bound is not served from this cache
+                other = [x for x in cases if x[1] != D][:2]
+                for q, h, c in other:
+                    a = dg.solve(q, h)
+                    _check(g, grp, q, h, a, c)
+            dg.cache_warm_hop([], 1, 0)
+        finally:
+            dg.close()
