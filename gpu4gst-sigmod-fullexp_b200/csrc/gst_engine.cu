@@ -582,8 +582,11 @@ struct Runner {
     // cache (exact everywhere; a member's distance 0 keeps its group out of the search).
     // With every group cached the query starts at the bounds pass; otherwise the search
     // runs for the other groups, its star bound already counting the cached ones.  A
-    // hop-bounded query uses the hop cache only when all its groups are cached for its
-    // bound: then every hop budget's table is gathered too.
+    // hop-bounded query takes its cached groups from the hop cache of its bound, every
+    // hop budget's table with them.  (The search's tentative star of D/2-edge paths may
+    // then count a cached distance of more edges and come out low; it only sets the
+    // search cutoff, which stays non-increasing, so every distance below the final
+    // cutoff is still exact and the bounds stay valid.)
     GroupVecs gv{};
     const uint32_t* hv[KMAX] = {};
     int n_cached = 0;
@@ -593,8 +596,7 @@ struct Runner {
     } else if (hop && q->hop_bound > 0 && !j->cache_dst && grp->hop_cache.cap > 0 &&
                grp->hop_cache.D == q->hop_bound) {
       for (int i = 0; i < q->k; i++) n_cached += (hv[i] = grp->hop_cache.vec(c.gid[i])) != nullptr;
-      if (n_cached < q->k) n_cached = 0;
-      for (int i = 0; i < q->k && n_cached; i++) gv.v[i] = hv[i] + (size_t)c.nhb * V;
+      for (int i = 0; i < q->k; i++) gv.v[i] = hv[i] ? hv[i] + (size_t)c.nhb * V : nullptr;
     }
     const bool cached = n_cached > 0;
     if (n_cached == q->k) {
@@ -621,7 +623,7 @@ struct Runner {
       if (hop)
         for (int h = 1; h <= c.nhb; h++) {
           GroupVecs gh{};
-          for (int i = 0; i < q->k; i++) gh.v[i] = hv[i] + (size_t)(h - 1) * V;
+          for (int i = 0; i < q->k; i++) gh.v[i] = hv[i] ? hv[i] + (size_t)(h - 1) * V : nullptr;
           k_gather_dist<<<eng->sssp_blocks, 256, 0, st>>>(
               m.dist_h + (size_t)(h - 1) * V * DIST_STRIDE, q->k, gh, g->V);
           cs.launches += 1;

@@ -157,8 +157,9 @@ gst_status gst_groups_cache_warm(gst_groups* grp, int32_t n, const int32_t* grou
 /* The same for queries with hop bound hop_bound (1..30): per group, the cheapest paths
  * of at most h edges to every vertex for every hop budget the engine bounds with
  * (4 x V x (min(hop_bound-1, 7) + 1) bytes per group).  A hop-bounded query with that
- * bound whose groups are all cached skips the distance search.  One hop bound at a
- * time: warming with another (or another max_bytes) drops the hop cache first. */
+ * bound whose groups are all cached skips the distance search; with some cached, the
+ * search runs for the others only.  One hop bound at a time: warming with another (or
+ * another max_bytes) drops the hop cache first. */
 gst_status gst_groups_cache_warm_hop(gst_groups* grp, int32_t n, const int32_t* group_ids,
                                      int32_t hop_bound, int64_t max_bytes, int32_t* n_cached);
 

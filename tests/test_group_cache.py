@@ -127,6 +127,13 @@ def test_hop_cache_matches_reference(engine):
                 qs = [q for q, _, _ in mine]
                 for (q, h, c), a in zip(mine, dg.solve_batch(qs, [D] * len(qs))):
                     _check(g, grp, q, h, a, c)
+                # a query with some groups cached searches for the others only
+                q, h, c = mine[0]
+                dg.cache_warm_hop([], D, 0)
+                assert dg.cache_warm_hop(list(q[:2]), D, per * len(gids)) == 2
+                a = dg.solve(q, h)
+                _check(g, grp, q, h, a, c)
+                assert len(q) > 2 and a.stats["sssp_relaxations"] > 0
                 # another bound is not served from this cache
                 other = [x for x in cases if x[1] != D][:2]
                 for q, h, c in other:
