@@ -595,6 +595,9 @@ __global__ void k_init(Ctx* ctxs, int nctx, DevGraph G, const int64_t* grp_ptr,
 //    the expand step snapshots the rows of the announced vertices and queues all
 //    their chunks, the relax step extends exactly those distances by one edge
 //    (rounds 1..D), so that the result is the same as one item per path.
+// Lane-local item word of the search: bits 0..7 the group mask (group-mask items) or
+// group index, 8..15 the round (hop-limited searches), 24..27 k, bit 30 SSSP_MASKED;
+// in the worklists bit 31 is CHUNK.
 constexpr uint32_t SSSP_MASKED = 0x40000000u;  // lane-local flag: a group-mask item
 constexpr int SSSP_U = 2;                      // edges per lane per round of the relax loop
 __global__ void __launch_bounds__(256, 4) k_sssp(Ctx* ctxs, int nctx, DevGraph G, int split) {
