@@ -69,6 +69,13 @@ SPECS = [
      "groups": {"kind": "zipf", "n": 1000, "s": 1.5, "smin": 2, "smax": 200, "seed": 92},
      "queries": [{"k": 6, "n": 20, "seed": 93, "hop": [None, 3]}],
      "solvers": ["PrunedDP++", "D-PrunedDP++"]},
+    # the largest query sizes (k = 7 runs in the default bench; 8 is the maximum)
+    {"name": "rmat4k_k7_k8",
+     "graph": {"kind": "rmat", "V": 4000, "E": 16000, "seed": 111},
+     "groups": {"kind": "zipf", "n": 300, "s": 1.5, "smin": 2, "smax": 120, "seed": 112},
+     "queries": [{"k": 7, "n": 16, "seed": 113, "hop": [None, 3]},
+                 {"k": 8, "n": 10, "seed": 114, "hop": [None, 3]}],
+     "solvers": ["PrunedDP++", "TrimCDP-multi-core-CPU", "D-PrunedDP++"]},
     # hop-bounded queries at a larger scale (the hop-limited lower bounds prune hard)
     {"name": "rmat50k_hop",
      "graph": {"kind": "rmat", "V": 50000, "E": 400000, "seed": 101},

@@ -24,7 +24,8 @@ def _check(g, grp, q, hop, a, expect):
         assert rc == 0, (q, hop, G.VERIFY_CODES[rc])
 
 
-@pytest.mark.parametrize("name", ["c1_ba20k_k3", "rmat3k_k4_k5", "rmat20k_k6", "rmat50k_hop"])
+@pytest.mark.parametrize("name", ["c1_ba20k_k3", "rmat3k_k4_k5", "rmat20k_k6", "rmat50k_hop",
+                                  "rmat4k_k7_k8"])
 def test_engine_matches_reference_golden(engine, name):
     fx = load_golden(name)
     g, grp = golden_inputs(fx)

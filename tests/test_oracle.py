@@ -16,7 +16,8 @@ def _ref_cost(c):
     return -1 if c >= REF_INF else c
 
 
-@pytest.mark.parametrize("name", ["c1_ba20k_k3", "rmat3k_k4_k5", "rmat20k_k6", "rmat50k_hop"])
+@pytest.mark.parametrize("name", ["c1_ba20k_k3", "rmat3k_k4_k5", "rmat20k_k6", "rmat50k_hop",
+                                  "rmat4k_k7_k8"])
 def test_oracle_matches_reference_golden(name):
     fx = load_golden(name)
     g, grp = golden_inputs(fx)
