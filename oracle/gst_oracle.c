@@ -27,9 +27,9 @@
  *                       (v,p2,d2), d2<=D-d, into max(d,d2) (:205-225), stop at
  *                       the first popped full-set state at any d<=D (:184-188),
  *                       parent walk (:231-257).
- *   oracle_hop_bound_check  not a reference algorithm: oracle_gst_hop pruned with
- *                       the engine's hop-bounded bounds, so that tests can check
- *                       that those bounds never remove an optimal tree.
+ *   oracle_hop_bound_check, oracle_nonhop_bound_check  not reference algorithms:
+ *                       the DPs above pruned with the engine's rules, so that tests
+ *                       can check that those rules never remove an optimal tree.
  *
  * Parity pin: tests/golden/ holds costs produced by the reference's own CPU
  * solvers (compiled unmodified under oracle/_ref by oracle/Makefile) on seeded
@@ -529,5 +529,165 @@ int oracle_hop_bound_check(int64_t V, const int64_t* beg, const int32_t* adj, co
   free(mask);
   free(dh);
   free(c);
+  return 0;
+}
+
+/* ---- check of the engine's unbounded pruning (not a reference algorithm) -----
+ * oracle_nonhop_bound_check runs the cost-ordered DP of oracle_gst_nonhop with the
+ * engine's rules against ub = the star bound min_v sum_i d_i(v) (a feasible cost):
+ *   a popped state (v, p, c) grows only if 2c <= ub, c + max_{i not in p} d_i(v) <= ub
+ *   and c + ceil(max(lb1, lb2) / 2) <= ub (tour bound, below);
+ *   a grown target (u, p, c') is written only if c' <= ub, c' + max_{i not in p} d_i(u)
+ *   <= ub and c' + ceil(lb2 / 2) <= ub (the O(k) half of the tour bound);
+ *   a merged state other than the full set is kept only if 3c <= 2ub;
+ * with Xb the missing groups, vv[i][j] = min over members m of group i of d_j(m),
+ * P(X, a, b) the cheapest group sequence from a to b visiting each group of X once
+ * (P(X, a, a) unbounded once X has two groups), W2(X, a) = min_b P(X, a, b),
+ *   lb1 = min_{a,b in Xb} d_a(v) + P(Xb, a, b) + d_b(v),
+ *   lb2 = max_{a in Xb} (d_a(v) + W2(Xb, a)) + min_{b in Xb} d_b(v).
+ * Equal costs to oracle_gst_nonhop on random instances check that these rules never
+ * remove an optimal tree.  Outputs: cost (-1 infeasible), star (-1 none), pops. */
+int oracle_nonhop_bound_check(int64_t V, const int64_t* beg, const int32_t* adj,
+                              const int32_t* w, const int64_t* grp_ptr, const int32_t* members,
+                              int32_t k, const int32_t* group_ids, int64_t* cost, int64_t* star,
+                              int64_t* pops) {
+  if (k < 1 || k > 8) return 1;
+  const int32_t W = 1 << k, FULL = W - 1;
+  uint32_t* mask = query_masks(V, grp_ptr, members, k, group_ids);
+  int64_t* d = (int64_t*)malloc(sizeof(int64_t) * (size_t)(V * k));  /* d[i * V + v] */
+  int64_t* c = (int64_t*)malloc(sizeof(int64_t) * (size_t)(V * W));
+  int64_t* P = (int64_t*)malloc(sizeof(int64_t) * (size_t)W * 64);   /* P[X][a][b] */
+  if (!mask || !d || !c || !P) return 2;
+  for (int32_t i = 0; i < k; i++) {
+    const int32_t g = group_ids[i];
+    oracle_sssp_groups(V, beg, adj, w, grp_ptr[g + 1] - grp_ptr[g], members + grp_ptr[g],
+                       d + (int64_t)i * V);
+  }
+  int64_t vv[8][8];
+  for (int32_t i = 0; i < k; i++)
+    for (int32_t j = 0; j < k; j++) {
+      vv[i][j] = ORACLE_INF;
+      const int32_t g = group_ids[i];
+      for (int64_t m = grp_ptr[g]; m < grp_ptr[g + 1]; m++)
+        if (d[(int64_t)j * V + members[m]] < vv[i][j]) vv[i][j] = d[(int64_t)j * V + members[m]];
+    }
+  for (int64_t x = 0; x < (int64_t)W * 64; x++) P[x] = ORACLE_INF;
+  for (int32_t X = 1; X <= FULL; X++)
+    for (int32_t a = 0; a < k; a++) {
+      if (!(X >> a & 1)) continue;
+      for (int32_t b = 0; b < k; b++) {
+        if (!(X >> b & 1)) continue;
+        int64_t val = ORACLE_INF;
+        if (X == (1 << a)) {
+          val = 0;
+        } else if (b != a) {
+          const int32_t prev = X ^ (1 << b);
+          for (int32_t j = 0; j < k; j++)
+            if ((prev >> j & 1) && P[(int64_t)prev * 64 + a * 8 + j] < ORACLE_INF &&
+                vv[j][b] < ORACLE_INF && P[(int64_t)prev * 64 + a * 8 + j] + vv[j][b] < val)
+              val = P[(int64_t)prev * 64 + a * 8 + j] + vv[j][b];
+        }
+        P[(int64_t)X * 64 + a * 8 + b] = val;
+      }
+    }
+  int64_t ub = ORACLE_INF;
+  for (int64_t v = 0; v < V; v++) {
+    int64_t s = 0;
+    for (int32_t i = 0; i < k && s < ORACLE_INF; i++)
+      s = d[(int64_t)i * V + v] >= ORACLE_INF ? ORACLE_INF : s + d[(int64_t)i * V + v];
+    if (s < ub) ub = s;
+  }
+  *star = ub < ORACLE_INF ? ub : -1;
+#define DV(i, v) (d[(int64_t)(i) * V + (v)])
+  for (int64_t i = 0; i < V * W; i++) c[i] = ORACLE_INF;
+  heap_t h = {0};
+  for (int64_t v = 0; v < V; v++)
+    for (int32_t i = 0; i < k; i++)
+      if (mask[v] >> i & 1) {
+        c[v * W + (1 << i)] = 0;
+        hitem it = {0, (int32_t)v, 1 << i, 0};
+        heap_push(&h, it);
+      }
+  int64_t npop = 0, best = -1;
+  while (h.n) {
+    hitem it = heap_pop(&h);
+    const int32_t v = it.v, p = it.p;
+    const int64_t cv = it.key;
+    if (cv != c[(int64_t)v * W + p]) continue;
+    npop++;
+    if (p == FULL) {
+      best = cv;
+      break;
+    }
+    const int32_t Xb = FULL ^ p;
+    /* bounds at the source */
+    int64_t one = 0, mind = ORACLE_INF, lb1 = ORACLE_INF, lb2 = 0;
+    for (int32_t i = 0; i < k; i++)
+      if (Xb >> i & 1) {
+        if (DV(i, v) > one) one = DV(i, v);
+        if (DV(i, v) < mind) mind = DV(i, v);
+      }
+    for (int32_t a = 0; a < k; a++) {
+      if (!(Xb >> a & 1)) continue;
+      int64_t w2 = ORACLE_INF;
+      for (int32_t b = 0; b < k; b++)
+        if ((Xb >> b & 1) && P[(int64_t)Xb * 64 + a * 8 + b] < w2) w2 = P[(int64_t)Xb * 64 + a * 8 + b];
+      const int64_t t2 = DV(a, v) + w2 + mind;
+      if (t2 > lb2) lb2 = t2;
+      for (int32_t b = 0; b < k; b++)
+        if (Xb >> b & 1) {
+          const int64_t t1 = DV(a, v) + P[(int64_t)Xb * 64 + a * 8 + b] + DV(b, v);
+          if (t1 < lb1) lb1 = t1;
+        }
+    }
+    const int64_t tb = lb1 > lb2 ? lb1 : lb2;
+    const int grow = 2 * cv <= ub && cv + one <= ub && cv + (tb + 1) / 2 <= ub;
+    if (grow)
+      for (int64_t e = beg[v]; e < beg[v + 1]; e++) {
+        const int32_t u = adj[e];
+        const int64_t nc = cv + w[e];
+        if (nc > ub || c[(int64_t)u * W + p] <= nc) continue;
+        /* the grow-time test on the target */
+        int64_t oneu = 0, mindu = ORACLE_INF, lb2u = 0;
+        for (int32_t i = 0; i < k; i++)
+          if (Xb >> i & 1) {
+            if (DV(i, u) > oneu) oneu = DV(i, u);
+            if (DV(i, u) < mindu) mindu = DV(i, u);
+          }
+        for (int32_t a = 0; a < k; a++) {
+          if (!(Xb >> a & 1)) continue;
+          int64_t w2 = ORACLE_INF;
+          for (int32_t b = 0; b < k; b++)
+            if ((Xb >> b & 1) && P[(int64_t)Xb * 64 + a * 8 + b] < w2) w2 = P[(int64_t)Xb * 64 + a * 8 + b];
+          const int64_t t2 = DV(a, u) + w2 + mindu;
+          if (t2 > lb2u) lb2u = t2;
+        }
+        if (nc + oneu > ub || nc + (lb2u + 1) / 2 > ub) continue;
+        c[(int64_t)u * W + p] = nc;
+        hitem ni = {nc, u, p, 0};
+        heap_push(&h, ni);
+      }
+    for (int32_t p2 = 1; p2 <= FULL; p2++) {
+      if (p2 & p) continue;
+      const int64_t c2 = c[(int64_t)v * W + p2];
+      if (c2 >= ORACLE_INF) continue;
+      const int32_t q = p | p2;
+      const int64_t nc = cv + c2;
+      if (q != FULL && 3 * nc > 2 * ub) continue;
+      if (c[(int64_t)v * W + q] > nc) {
+        c[(int64_t)v * W + q] = nc;
+        hitem ni = {nc, v, q, 0};
+        heap_push(&h, ni);
+      }
+    }
+  }
+#undef DV
+  *cost = best;
+  *pops = npop;
+  free(h.a);
+  free(mask);
+  free(d);
+  free(c);
+  free(P);
   return 0;
 }

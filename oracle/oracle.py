@@ -38,6 +38,8 @@ def lib():
                                         vp]
         _lib.oracle_hop_bound_check.argtypes = [C.c_int64, vp, vp, vp, vp, vp, C.c_int32, vp,
                                                 C.c_int32, vp, vp, vp]
+        _lib.oracle_nonhop_bound_check.argtypes = [C.c_int64, vp, vp, vp, vp, vp, C.c_int32,
+                                                   vp, vp, vp, vp]
     return _lib
 
 
@@ -90,6 +92,20 @@ def gst_nonhop(g, groups, group_ids):
 def gst_hop(g, groups, group_ids, hop_bound: int):
     """Exact optimum of the hop-bounded DP of D-PrunedDP++ (cost -1 = infeasible)."""
     return _solve(g, groups, group_ids, hop_bound)
+
+
+def nonhop_bound_check(g, groups, group_ids):
+    """The unbounded DP pruned with the engine's rules (2c <= ub to grow, 3c <= 2ub to
+    keep a merge, one-label and tour bounds at the source, the one-label bound and the
+    O(k) tour bound on a grown target) against the star bound; its cost must equal
+    gst_nonhop's.  Returns {cost, star (-1: none), pops}."""
+    gid = np.ascontiguousarray(group_ids, dtype=np.int32)
+    cost, star, pops = C.c_int64(), C.c_int64(), C.c_int64()
+    rc = lib().oracle_nonhop_bound_check(g.V, _p(g.beg_pos), _p(g.adj), _p(g.weight),
+                                         _p(groups.grp_ptr), _p(groups.members), gid.shape[0],
+                                         _p(gid), C.byref(cost), C.byref(star), C.byref(pops))
+    assert rc == 0, f"oracle failed rc={rc}"
+    return {"cost": cost.value, "star": star.value, "pops": pops.value}
 
 
 def hop_bound_check(g, groups, group_ids, hop_bound: int):

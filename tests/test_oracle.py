@@ -97,3 +97,31 @@ def test_hop_budget_bounds_keep_the_optimum():
             assert chk["pops"] <= plain["pops"]
             n += 1
     assert n == 96
+
+
+def test_unbounded_pruning_rules_keep_the_optimum():
+    """The engine's unbounded pruning: grow only states with 2c <= ub that pass the
+    one-label and tour bounds, write a grown target only if its one-label bound and
+    the O(k) half of its tour bound pass, keep a merged non-full state only if
+    3c <= 2ub.  Applied to the cost-ordered DP against the star bound, they find the
+    unpruned optimum on random instances (k up to 8)."""
+    rng = np.random.default_rng(77)
+    n = 0
+    for t in range(16):
+        if t % 2:
+            g = G.synth_rmat(int(rng.integers(300, 1500)), int(rng.integers(1500, 8000)),
+                             int(rng.integers(1, 1 << 30)))
+        else:
+            g = G.synth_ba(int(rng.integers(300, 1500)), int(rng.integers(1, 4)),
+                           int(rng.integers(1, 1 << 30)))
+        grp = G.synth_groups_zipf(g.V, 40, 1.5, 1, 30, int(rng.integers(1, 1 << 30)))
+        for _ in range(4):
+            k = int(rng.integers(2, 9))
+            q = G.synth_queries(grp.n_groups, 1, k, int(rng.integers(1, 1 << 30)))[0]
+            plain = O.gst_nonhop(g, grp, q)
+            chk = O.nonhop_bound_check(g, grp, q)
+            assert chk["cost"] == plain["cost"], (t, k, chk, plain["cost"])
+            if chk["star"] >= 0:
+                assert chk["star"] >= plain["cost"] >= 0
+            n += 1
+    assert n == 64
