@@ -417,27 +417,35 @@ int oracle_gst_hop(int64_t V, const int64_t* beg, const int32_t* adj, const int3
 }
 
 /* ---- check of the engine's hop-bounded pruning (not a reference algorithm) ----
- * oracle_hop_bound_check runs the cost-ordered hop DP of oracle_gst_hop, but keeps
- * no grown or merged state (v, p, d) of cost c with
- *     c + max_{i not in p} d_i^{<=D-d}(v) > ub,
- * d^{<=h} being the cheapest paths of at most h edges (h synchronous rounds here)
- * and ub the cheapest star of paths of at most D/2 edges (a tree of diameter <= D),
- * or no bound when no such star exists.  These are the bounds the engine's
- * hop-bounded queries prune with (it keeps c + lb <= ub + 1, a looser test).  The
- * tests compare the cost with oracle_gst_hop's: equal costs on random instances
- * check that the bounds never remove an optimal tree.
- * Outputs: cost (-1 infeasible), star (-1 none), pops (states settled). */
+ * oracle_hop_bound_check runs the cost-ordered hop DP of oracle_gst_hop with the rules
+ * the engine prunes hop-bounded queries with, against ub = the cheapest star of paths
+ * of at most D/2 edges (a tree of diameter <= D), or no bound when none exists.  With
+ * d^{<=h} the cheapest paths of at most h edges (h synchronous rounds here), a state
+ * (v, p, d) of cost c, Xb the missing groups and dl_i = d_i^{<=D-d}(v):
+ *   it grows (to height d + 1 < = D) only if 2c <= ub, c + max_{i in Xb} dl_i <= ub and
+ *   c + ceil(max(lb1, lb2) / 2) <= ub, lb1 and lb2 the tour bounds below on dl;
+ *   a grown target (u, p, d + 1) is written only if its cost c' keeps c' < ub + 1,
+ *   c' + max dl_i(u) <= ub and c' + ceil(lb2(u) / 2) <= ub;
+ *   a merged state other than the full set is kept only if 3c <= 2ub.
+ * The tour bounds use group distances vv[i][j] = min over members m of group i of
+ * d_j^{<=D}(m) (the tree paths between groups have at most D edges):
+ *   lb1 = min_{a,b in Xb} dl_a + P(Xb, a, b) + dl_b,
+ *   lb2 = max_{a in Xb} (dl_a + min_b P(Xb, a, b)) + min_{b in Xb} dl_b.
+ * The engine keeps c + lb <= ub + 1 (its bound is the star plus one), a looser test.
+ * Equal costs to oracle_gst_hop on random instances check that the rules never remove
+ * an optimal tree.  Outputs: cost (-1 infeasible), star (-1 none), pops. */
 int oracle_hop_bound_check(int64_t V, const int64_t* beg, const int32_t* adj, const int32_t* w,
                            const int64_t* grp_ptr, const int32_t* members, int32_t k,
                            const int32_t* group_ids, int32_t D, int64_t* cost, int64_t* star,
                            int64_t* pops) {
-  if (k < 1 || k > 16 || D < 0 || D > 64) return 1;
+  if (k < 1 || k > 8 || D < 0 || D > 64) return 1;
   const int32_t W = 1 << k, FULL = W - 1, DD = D + 1;
   const int64_t S = V * W * DD;
   uint32_t* mask = query_masks(V, grp_ptr, members, k, group_ids);
   int64_t* dh = (int64_t*)malloc(sizeof(int64_t) * (size_t)(V * k * DD));
   int64_t* c = (int64_t*)malloc(sizeof(int64_t) * (size_t)S);
-  if (!mask || !dh || !c) return 2;
+  int64_t* P = (int64_t*)malloc(sizeof(int64_t) * (size_t)W * 64);  /* P[X][a][b] */
+  if (!mask || !dh || !c || !P) return 2;
   /* d^{<=h}: round h extends the paths of round h - 1 by one edge */
   for (int64_t v = 0; v < V; v++)
     for (int32_t i = 0; i < k; i++) dh[v * k + i] = (mask[v] >> i & 1) ? 0 : ORACLE_INF;
@@ -453,28 +461,72 @@ int oracle_hop_bound_check(int64_t V, const int64_t* beg, const int32_t* adj, co
             cur[(int64_t)adj[e] * k + i] = x;
         }
   }
-  int64_t ub = ORACLE_INF;
-  {
-    const int64_t* half = dh + (int64_t)(D / 2) * V * k;
-    for (int64_t v = 0; v < V; v++) {
-      int64_t s = 0;
-      for (int32_t i = 0; i < k && s < ORACLE_INF; i++)
-        s = half[v * k + i] >= ORACLE_INF ? ORACLE_INF : s + half[v * k + i];
-      if (s < ub) ub = s;
+#define DH(h, v, i) (dh[((int64_t)(h) * V + (v)) * k + (i)])
+  int64_t vv[8][8];
+  for (int32_t i = 0; i < k; i++)
+    for (int32_t j = 0; j < k; j++) {
+      vv[i][j] = ORACLE_INF;
+      const int32_t g = group_ids[i];
+      for (int64_t m = grp_ptr[g]; m < grp_ptr[g + 1]; m++)
+        if (DH(D, members[m], j) < vv[i][j]) vv[i][j] = DH(D, members[m], j);
     }
+  for (int64_t x = 0; x < (int64_t)W * 64; x++) P[x] = ORACLE_INF;
+  for (int32_t X = 1; X <= FULL; X++)
+    for (int32_t a = 0; a < k; a++) {
+      if (!(X >> a & 1)) continue;
+      for (int32_t b = 0; b < k; b++) {
+        if (!(X >> b & 1)) continue;
+        int64_t val = ORACLE_INF;
+        if (X == (1 << a)) {
+          val = 0;
+        } else if (b != a) {
+          const int32_t prev = X ^ (1 << b);
+          for (int32_t j = 0; j < k; j++)
+            if ((prev >> j & 1) && P[(int64_t)prev * 64 + a * 8 + j] < ORACLE_INF &&
+                vv[j][b] < ORACLE_INF && P[(int64_t)prev * 64 + a * 8 + j] + vv[j][b] < val)
+              val = P[(int64_t)prev * 64 + a * 8 + j] + vv[j][b];
+        }
+        P[(int64_t)X * 64 + a * 8 + b] = val;
+      }
+    }
+  int64_t ub = ORACLE_INF;
+  for (int64_t v = 0; v < V; v++) {
+    int64_t sum = 0;
+    for (int32_t i = 0; i < k && sum < ORACLE_INF; i++)
+      sum = DH(D / 2, v, i) >= ORACLE_INF ? ORACLE_INF : sum + DH(D / 2, v, i);
+    if (sum < ub) ub = sum;
   }
   *star = ub < ORACLE_INF ? ub : -1;
+  /* the one-label bound, lb2 and (with `both`) lb1 of state (v, p) at height d */
+  int64_t one, lb1, lb2;
+#define BOUNDS(v, p, d, both)                                                          \
+  do {                                                                                 \
+    const int32_t xb_ = FULL ^ (p), h_ = D - (d);                                      \
+    int64_t mind_ = ORACLE_INF;                                                        \
+    one = 0;                                                                           \
+    lb1 = ORACLE_INF;                                                                  \
+    lb2 = 0;                                                                           \
+    for (int32_t i_ = 0; i_ < k; i_++)                                                 \
+      if (xb_ >> i_ & 1) {                                                             \
+        if (DH(h_, v, i_) > one) one = DH(h_, v, i_);                                  \
+        if (DH(h_, v, i_) < mind_) mind_ = DH(h_, v, i_);                              \
+      }                                                                                \
+    for (int32_t a_ = 0; a_ < k; a_++) {                                               \
+      if (!(xb_ >> a_ & 1)) continue;                                                  \
+      int64_t w2_ = ORACLE_INF;                                                        \
+      for (int32_t b_ = 0; b_ < k; b_++)                                               \
+        if (xb_ >> b_ & 1) {                                                           \
+          const int64_t pab_ = P[(int64_t)xb_ * 64 + a_ * 8 + b_];                     \
+          if (pab_ < w2_) w2_ = pab_;                                                  \
+          if (both && DH(h_, v, a_) + pab_ + DH(h_, v, b_) < lb1)                      \
+            lb1 = DH(h_, v, a_) + pab_ + DH(h_, v, b_);                                \
+        }                                                                              \
+      if (DH(h_, v, a_) + w2_ + mind_ > lb2) lb2 = DH(h_, v, a_) + w2_ + mind_;        \
+    }                                                                                  \
+  } while (0)
   for (int64_t i = 0; i < S; i++) c[i] = ORACLE_INF;
   heap_t h = {0};
 #define IDX(v, p, d) (((int64_t)(v) * W + (p)) * DD + (d))
-  /* lower bound of state (v, p, d): the missing groups within the budget D - d */
-#define LB(v, p, d, out)                                                       \
-  do {                                                                         \
-    const int64_t* row_ = dh + ((int64_t)(D - (d)) * V + (v)) * k;             \
-    (out) = 0;                                                                 \
-    for (int32_t i_ = 0; i_ < k; i_++)                                         \
-      if (!((p) >> i_ & 1) && row_[i_] > (out)) (out) = row_[i_];              \
-  } while (0)
   for (int64_t v = 0; v < V; v++)
     for (int32_t i = 0; i < k; i++)
       if (mask[v] >> i & 1) {
@@ -493,16 +545,17 @@ int oracle_hop_bound_check(int64_t V, const int64_t* beg, const int32_t* adj, co
       best = cv;
       break;
     }
-    if (d < D)
+    BOUNDS(v, p, d, 1);
+    const int64_t tb = lb1 > lb2 ? lb1 : lb2;
+    if (d < D && 2 * cv <= ub && cv + one <= ub && cv + (tb + 1) / 2 <= ub)
       for (int64_t e = beg[v]; e < beg[v + 1]; e++) {
         const int64_t t = IDX(adj[e], p, d + 1), nc = cv + w[e];
-        int64_t lb;
-        LB(adj[e], p, d + 1, lb);
-        if (c[t] > nc && nc + lb <= ub) {
-          c[t] = nc;
-          hitem ni = {nc, adj[e], p, d + 1};
-          heap_push(&h, ni);
-        }
+        if (nc > ub || c[t] <= nc) continue;
+        BOUNDS(adj[e], p, d + 1, 0);
+        if (nc + one > ub || nc + (lb2 + 1) / 2 > ub) continue;
+        c[t] = nc;
+        hitem ni = {nc, adj[e], p, d + 1};
+        heap_push(&h, ni);
       }
     for (int32_t p2 = 1; p2 <= FULL; p2++) {
       if (p2 & p) continue;
@@ -511,9 +564,8 @@ int oracle_hop_bound_check(int64_t V, const int64_t* beg, const int32_t* adj, co
         if (c2 >= ORACLE_INF) continue;
         const int32_t nd = d > d2 ? d : d2, q = p | p2;
         const int64_t t = IDX(v, q, nd), nc = cv + c2;
-        int64_t lb = 0;
-        if (q != FULL) LB(v, q, nd, lb);
-        if (c[t] > nc && nc + lb <= ub) {
+        if (q != FULL && 3 * nc > 2 * ub) continue;
+        if (c[t] > nc) {
           c[t] = nc;
           hitem ni = {nc, v, q, nd};
           heap_push(&h, ni);
@@ -521,14 +573,16 @@ int oracle_hop_bound_check(int64_t V, const int64_t* beg, const int32_t* adj, co
       }
     }
   }
-#undef LB
 #undef IDX
+#undef BOUNDS
+#undef DH
   *cost = best;
   *pops = npop;
   free(h.a);
   free(mask);
   free(dh);
   free(c);
+  free(P);
   return 0;
 }
 

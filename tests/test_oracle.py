@@ -72,9 +72,11 @@ def test_oracle_sssp_matches_dp_singletons():
 def test_hop_budget_bounds_keep_the_optimum():
     """The engine prunes hop-bounded states with the distances within each state's
     remaining hop budget (a state of height d reaches every missing group within
-    D - d edges) against the star of D/2-edge paths.  The DP pruned that way finds
-    the same optimum as the unpruned one on random instances, the star is a
-    feasible cost (never below the optimum), and the pruning settles fewer states."""
+    D - d edges), in the one-label and tour bounds, with the grow (2c <= ub) and
+    merge (3c <= 2ub) cost rules and the grow-time test on targets, against the star
+    of D/2-edge paths.  The DP pruned that way finds the same optimum as the unpruned
+    one on random instances (k up to 8, D up to 6), the star is a feasible cost
+    (never below the optimum), and the pruning settles fewer states."""
     rng = np.random.default_rng(2024)
     n = 0
     for t in range(24):
@@ -86,7 +88,7 @@ def test_hop_budget_bounds_keep_the_optimum():
                            int(rng.integers(1, 1 << 30)))
         grp = G.synth_groups_zipf(g.V, 40, 1.5, 1, 30, int(rng.integers(1, 1 << 30)))
         for _ in range(4):
-            k = int(rng.integers(2, 6))
+            k = int(rng.integers(2, 9))
             D = int(rng.integers(1, 7))
             q = G.synth_queries(grp.n_groups, 1, k, int(rng.integers(1, 1 << 30)))[0]
             plain = O.gst_hop(g, grp, q, D)
