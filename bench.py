@@ -72,6 +72,21 @@ WORKLOADS = {
 }
 
 
+def mix_queries(pools, hop, kmax=8):
+    """A seeded shuffle of the query pools (one per k), a seeded fraction of them with
+    hop bound D; queries of more than kmax groups stay unbounded.  hop = (D, fraction,
+    seed).  Returns (queries, hops), hops[i] None for an unbounded query."""
+    import numpy as np
+    D, frac, hseed = hop
+    allq = [q for p in pools for q in p]
+    rng = np.random.default_rng(hseed)
+    order = rng.permutation(len(allq))
+    queries = [allq[i] for i in order]
+    hops = [D if x < frac else None for x in rng.random(len(queries))]
+    hops = [h if len(q) <= kmax else None for q, h in zip(queries, hops)]
+    return queries, hops
+
+
 def make_workload(key):
     import gst_b200 as G
     w = WORKLOADS[key]
@@ -88,16 +103,7 @@ def make_workload(key):
     pools = [G.synth_queries(grp.n_groups, n, k, s) for k, n, s in w["queries"]]
     queries = []
     if "hop" in w:
-        # seeded shuffle of the k classes, and a seeded half of them hop-bounded
-        import numpy as np
-        D, frac, hseed = w["hop"]
-        allq = [q for p in pools for q in p]
-        rng = np.random.default_rng(hseed)
-        order = rng.permutation(len(allq))
-        queries = [allq[i] for i in order]
-        hops = [D if x < frac else None for x in rng.random(len(queries))]
-        kmax = w.get("hop_kmax", 8)
-        hops = [h if len(q) <= kmax else None for q, h in zip(queries, hops)]
+        queries, hops = mix_queries(pools, w["hop"], w.get("hop_kmax", 8))
         return w, g, grp, queries, hops
     # interleave the k classes: k5, k7, k5, k7, ...
     for i in range(max(len(p) for p in pools)):
