@@ -74,6 +74,11 @@ def build(force: bool = False, verbose_ptxas: bool = False, checked: bool = Fals
         if force or _stale(exe, [cli_src, LIB] + hdrs):
             _run([CXX, "-O2", "-std=c++17", "-I", INC, cli_src, "-o", exe, "-L", HERE,
                   "-lgst_b200", f"-Wl,-rpath,{HERE}", "-Wl,-rpath,$ORIGIN"])
+    gen_srcs = [os.path.join(CSRC, f) for f in ("gst_gen.cpp", "gst_synth.cpp", "gst_io.cpp")]
+    gen = os.path.join(HERE, "gst_gen")
+    if all(os.path.exists(f) for f in gen_srcs) and (force or _stale(gen, gen_srcs + hdrs)):
+        # standalone: the generator and IO sources only, no engine library
+        _run([CXX, "-O3", "-std=c++17", "-fopenmp", "-I", INC, *gen_srcs, "-o", gen])
     return LIB
 
 

@@ -59,7 +59,8 @@ constexpr int DIST_STRIDE = 8;    // int32 one-label distances per vertex row
 // being built (one k_sssp pass over the distance rows, then the control block).
 enum Phase : uint32_t { PH_SSSP = 0, PH_PREP = 1, PH_DP = 2, PH_DONE = 3, PH_ERROR = 4 };
 enum ErrBits : uint32_t { ERR_QCAP = 1, ERR_FARCAP = 2, ERR_ROWCAP = 4, ERR_TIMEOUT = 8,
-                          ERR_EXTRACT = 16, ERR_BOUNDS = 32 };
+                          ERR_EXTRACT = 16, ERR_BOUNDS = 32, ERR_POOL = 64 };
+constexpr uint32_t ROW_NONE = 0xFFFFFFFFu;
 enum CtrlMode : int { CTRL_SSSP = 0, CTRL_DP_ROWS = 1, CTRL_DP_GROW = 2 };
 
 // Light-edge index: per vertex, the number of edges of weight <= widx_threshold(t)
@@ -112,7 +113,10 @@ __device__ __forceinline__ int64_t count_upto(const DevGraph& G, uint32_t v, int
 // query starts; the rest are updated by the control kernel between launches and
 // by atomics inside the level kernels.
 struct Ctx {
-  uint64_t* table;
+  uint64_t* table;     // state rows: the dense slab (V rows), or the row pool (pool_cap rows)
+  uint32_t* rowmap;    // row pool: vertex -> its pool row (ROW_NONE: none yet); nullptr: dense
+  uint32_t pool_cap;   // rows of the pool
+  uint32_t pool_n;     // pool rows handed out (may exceed pool_cap: ERR_POOL)
   uint32_t* dist;
   uint32_t* rowbits;
   uint32_t* fm[2];     // group-mask frontier (one byte per vertex, four to a word): the
@@ -188,6 +192,38 @@ __device__ __forceinline__ bool in_bounds(Ctx* c, bool ok, uint32_t site) {
 #else
 #define in_bounds(c, ok, site) true
 #endif
+
+// ---- state rows ----------------------------------------------------------------------
+// A query's states live in rows of RW cells, one row per vertex that holds any finite
+// state.  Dense layout (rowmap == nullptr): row v at table + v * RW, all V rows.  Row
+// pool: a vertex gets a row from a pool of pool_cap rows (pre-filled with unreached
+// cells) the first time one of its states is written; rowmap[v] names it.  A query
+// writes rows for a small share of the vertices (its pruned DP settles few states), so
+// the pool holds its table in a fraction of the dense slab's memory, and clearing it
+// for the next query touches only the rows the last one used.
+__device__ __forceinline__ uint64_t* row_of(const Ctx* c, uint32_t v) {
+  if (!c->rowmap) return c->table + (uint64_t)v * (uint64_t)c->RW;
+  const uint32_t r = __ldcg(&c->rowmap[v]);
+  return r == ROW_NONE ? nullptr : c->table + (uint64_t)r * (uint64_t)c->RW;
+}
+// Row of v given its rowmap entry r (as loaded by the caller), taking a pool row when v
+// has none; nullptr when the pool is exhausted (ERR_POOL: the query is re-run with a
+// larger pool).  Two lanes taking a row for the same vertex at once both draw a pool
+// index; the one whose compare-and-swap loses uses the winner's row, and its own index
+// stays unused.
+__device__ __forceinline__ uint64_t* row_take(Ctx* c, uint32_t v, uint32_t r) {
+  if (!c->rowmap) return c->table + (uint64_t)v * (uint64_t)c->RW;
+  if (r == ROW_NONE) {
+    const uint32_t mine = atomicAdd(&c->pool_n, 1u);
+    if (mine >= c->pool_cap) {
+      atomicOr(&c->error, (uint32_t)ERR_POOL);
+      return nullptr;
+    }
+    const uint32_t old = atomicCAS(&c->rowmap[v], ROW_NONE, mine);
+    r = old == ROW_NONE ? mine : old;
+  }
+  return c->table + (uint64_t)r * (uint64_t)c->RW;
+}
 
 // One-label distances of v within the hop budget h of a hop-bounded query: d_i^{<=h}(v),
 // the cheapest paths of at most h edges.  A state of height d (a tree hanging from v
@@ -548,8 +584,9 @@ __global__ void k_init(Ctx* ctxs, int nctx, DevGraph G, const int64_t* grp_ptr,
         const uint32_t v = (uint32_t)members[j];
         if (!in_bounds(c, v < G.V && i < c->k, 1)) continue;
         const uint64_t cell0 = pack_cell(0, PEND | LEAF);
-        atomicMin((unsigned long long*)&c->table[(uint64_t)v * c->RW + (1u << i)],
-                  (unsigned long long)cell0);
+        uint64_t* row = row_take(c, v, c->rowmap ? __ldcg(&c->rowmap[v]) : 0u);
+        if (!row) continue;
+        atomicMin((unsigned long long*)&row[1u << i], (unsigned long long)cell0);
         mark_row(c, v);
         if (c->phase == PH_SSSP) {
           const uint32_t old = atomicMin(&c->dist[(uint64_t)v * DIST_STRIDE + i], 0u);
@@ -908,9 +945,9 @@ __global__ void __launch_bounds__(256, 3) k_grow(Ctx* ctxs, int nctx, DevGraph G
       const uint32_t p = pd & 0xFFFFu, d = pd >> 16;
       const bool ok = in_bounds(c, v < G.V && p < (uint32_t)c->W && d < (uint32_t)c->DD, 5);
       const int64_t b0 = ok ? G.beg[v] : 0, b1 = ok ? G.beg[v + 1] : 0;
-      const uint64_t cell = ok ? __ldcg((const unsigned long long*)&c->table[(uint64_t)v * c->RW +
-                                                                           ((uint64_t)d << c->k) + p])
-                               : 0ull;
+      const uint64_t* srow = ok ? row_of(c, v) : nullptr;
+      const uint64_t cell = srow ? __ldcg((const unsigned long long*)&srow[((uint64_t)d << c->k) + p])
+                                 : CELL_INF;
       bound = c->hop ? __ldcg(&c->ub_cell) : __ldcg(&c->ub);
       // a work item always names a state that holds a finite cost
       const bool src_ok = !ok || in_bounds(c, cost_of(cell) != COST_INF, 12);
@@ -958,6 +995,7 @@ __global__ void __launch_bounds__(256, 3) k_grow(Ctx* ctxs, int nctx, DevGraph G
       // (32 bytes per vertex) stay in L2 while its state table does not, so the
       // tests come first and only edges that pass them read a table cell.
       uint4 da[RELAX_U], db[RELAX_U];
+      uint32_t rm[RELAX_U];  // the target's pool row (row pool), loaded with its distances
 #pragma unroll
       for (int x = 0; x < RELAX_U; x++) {
         Ctx* c = ctxs + x_qi[x];
@@ -967,6 +1005,7 @@ __global__ void __launch_bounds__(256, 3) k_grow(Ctx* ctxs, int nctx, DevGraph G
         const bool keep = hop ? (nc < x_bound[x]) : (nc <= x_bound[x]);
         const uint32_t d = (x_pd[x] >> 16) + (uint32_t)hop;
         ok[x] = ok[x] && in_bounds(c, u < G.V, 7) && keep && in_bounds(c, d < (uint32_t)c->DD, 11);
+        rm[x] = ok[x] && c->rowmap ? __ldcg(&c->rowmap[u]) : ROW_NONE;
         da[x] = db[x] = make_uint4(0, 0, 0, 0);
         if (ok[x] && c->use_lb) {
           if (hop && c->sssp_hops) {
@@ -1016,9 +1055,12 @@ __global__ void __launch_bounds__(256, 3) k_grow(Ctx* ctxs, int nctx, DevGraph G
             if ((uint64_t)nc + (lb2 + 1) / 2 > (uint64_t)x_bound[x]) ok[x] = false;
           }
         }
-        cur[x] = ok[x] ? __ldcg((const unsigned long long*)&c->table[(uint64_t)u * c->RW +
-                                                                     ((uint64_t)d << c->k) + p])
-                       : 0ull;
+        // the target's cell: unreached when its vertex has no pool row yet
+        const bool has_row = ok[x] && (!c->rowmap || rm[x] != ROW_NONE);
+        const uint64_t off = ((uint64_t)d << c->k) + p;
+        cur[x] = has_row ? __ldcg((const unsigned long long*)&(c->rowmap ? c->table + (uint64_t)rm[x] * c->RW
+                                                                         : c->table + (uint64_t)u * c->RW)[off])
+                         : CELL_INF;
       }
 #pragma unroll
       for (int x = 0; x < RELAX_U; x++) {
@@ -1027,10 +1069,12 @@ __global__ void __launch_bounds__(256, 3) k_grow(Ctx* ctxs, int nctx, DevGraph G
         bool dirty = false;
         if (ok[x] && pack_cell(nc, PEND | x_v[x]) < cur[x]) {
           const uint32_t p = x_pd[x] & 0xFFFFu, d = (x_pd[x] >> 16) + (uint32_t)c->hop;
-          unsigned long long* tp =
-              (unsigned long long*)&c->table[(uint64_t)u * c->RW + ((uint64_t)d << c->k) + p];
-          const uint64_t old = atomicMin(tp, (unsigned long long)pack_cell(nc, PEND | x_v[x]));
-          dirty = cost_of(old) > nc;
+          uint64_t* row = row_take(c, u, rm[x]);
+          if (row) {
+            unsigned long long* tp = (unsigned long long*)&row[((uint64_t)d << c->k) + p];
+            const uint64_t old = atomicMin(tp, (unsigned long long)pack_cell(nc, PEND | x_v[x]));
+            dirty = cost_of(old) > nc;
+          }
         }
         warp_mark_row(ctxs, x_qi[x], dirty, u);
       }
@@ -1078,7 +1122,14 @@ __global__ void __launch_bounds__(256, 4) k_rows(Ctx* ctxs, int nctx, DevGraph G
     const int RW = c->RW, W = c->W, DD = c->DD, k = c->k, D = c->D, hop = c->hop;
     (void)W;
     const uint32_t full = (uint32_t)c->full;
-    unsigned long long* row = (unsigned long long*)&c->table[(uint64_t)v * RW];
+    unsigned long long* row = (unsigned long long*)row_of(c, v);
+    if (row == nullptr) {  // never for a dirty row: a row is taken before its first write
+      if (lane == 0) {
+        atomicAnd(&c->rowbits[v >> 5], ~(1u << (v & 31)));
+        atomicOr(&c->error, (uint32_t)ERR_BOUNDS);
+      }
+      continue;
+    }
     // load the row; list its pending cells (plist) and its finite cells (flist)
     int np = 0, nf = 0;
     for (int i0 = 0; i0 < RW; i0 += 32) {
@@ -1645,7 +1696,8 @@ __global__ void k_extract(Ctx* ctxs, int nctx, DevGraph G) {
     const uint32_t v = (uint32_t)(idx / RW);
     const uint32_t r = (uint32_t)(idx - (uint64_t)v * RW);
     const uint32_t p = r & (uint32_t)c->full, d = r >> k;
-    const uint64_t cell = c->table[idx];
+    const uint64_t* vrow = row_of(c, v);
+    const uint64_t cell = vrow ? vrow[r] : CELL_INF;
     const uint32_t par = (uint32_t)cell & ~PEND;
     if (cost_of(cell) == COST_INF) {  // a parent pointer never leads to an unreached state
       c->error |= ERR_EXTRACT;

@@ -47,10 +47,12 @@ using Clock = std::chrono::steady_clock;
 struct SlotMem {
   void* base = nullptr;
   size_t bytes = 0;
-  size_t rw = 0;          // cells per row the slab holds
+  size_t table_bytes = 0; // state rows (the row pool) of the slot
+  size_t table_dirty = 0; // bytes at the table's start that may hold written cells
   uint32_t cap = 0;       // near-list capacity (items)
   uint32_t farcap = 0;    // far-list capacity (0 when the frontier has one bucket)
   uint64_t* table = nullptr;
+  uint32_t* rowmap = nullptr;  // vertex -> pool row
   uint32_t* dist = nullptr;
   uint32_t* rowbits = nullptr;
   uint32_t* fm[2] = {nullptr, nullptr};
@@ -72,20 +74,38 @@ constexpr uint32_t kStackCap = 1u << 18;
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-// Lay out (or, with base == nullptr, only size) a slot of V rows of rw cells.
-size_t carve_slot(SlotMem& m, unsigned char* base, int64_t V, size_t rw, uint32_t cap,
-                  uint32_t farcap, int nhb) {
+// Frontier bytes of the distance search: one per vertex (four to a word), padded to
+// whole 16-byte words.
+size_t fm_bytes(int64_t V) { return ((size_t)V + 15) / 16 * 16; }
+
+// Rows of a query's row pool: an eighth of the vertices (at least 64k rows), four times
+// more per capacity retry.  A query writes rows for a few percent of the vertices (its
+// pruning keeps the DP near the optimal trees).  A pool of half the vertices or more
+// becomes the dense layout (one row per vertex, no map): small graphs, last retries.
+uint32_t pool_rows(int64_t V, int boost) {
+  uint64_t r = std::max<uint64_t>(1u << 16, (uint64_t)V / 8);
+  for (int i = 0; i < boost; i++) r *= 4;
+  return r * 2 >= (uint64_t)V ? (uint32_t)V : (uint32_t)r;
+}
+
+// Lay out (or, with base == nullptr, only size) a slot of V vertices: a row pool of
+// `rows` rows of rw cells and the per-vertex buffers.
+size_t carve_slot(SlotMem& m, unsigned char* base, int64_t V, size_t rw, uint32_t rows,
+                  uint32_t cap, uint32_t farcap, int nhb) {
   size_t off = 0;
   auto take = [&](size_t n) {
     unsigned char* p = base ? base + off : nullptr;
     off = align256(off + n);
     return p;
   };
-  m.table = (uint64_t*)take((size_t)V * rw * 8);
+  m.table_bytes = (size_t)rows * rw * 8;
+  m.table_dirty = m.table_bytes;  // fresh memory: cleared before first use
+  m.table = (uint64_t*)take(m.table_bytes);
+  m.rowmap = (uint32_t*)take((size_t)V * 4);
   m.dist = (uint32_t*)take((size_t)V * DIST_STRIDE * 4);
   m.rowbits = (uint32_t*)take(((size_t)V + 31) / 32 * 4);
-  m.fm[0] = (uint32_t*)take(((size_t)V + 3) / 4 * 4);
-  m.fm[1] = (uint32_t*)take(((size_t)V + 3) / 4 * 4);
+  m.fm[0] = (uint32_t*)take(fm_bytes(V));
+  m.fm[1] = (uint32_t*)take(fm_bytes(V));
   m.snap = (uint32_t*)take((size_t)V * DIST_STRIDE * 4);
   m.dist_h = (uint32_t*)take((size_t)nhb * (size_t)V * DIST_STRIDE * 4);
   m.nhb = nhb;
@@ -97,7 +117,6 @@ size_t carve_slot(SlotMem& m, unsigned char* base, int64_t V, size_t rw, uint32_
   m.rows = (uint32_t*)take((size_t)V * 4);
   m.out = (int32_t*)take((size_t)kOutCap * 12);
   m.stack = (uint64_t*)take((size_t)kStackCap * 8);
-  m.rw = rw;
   m.cap = cap;
   m.farcap = farcap;
   m.rowcap = (uint32_t)V;
@@ -138,6 +157,8 @@ struct gst_engine {
   int sms = 148;
   int grow_blocks = 0, sssp_blocks = 0;
   std::vector<std::pair<uint64_t, int>> rows_occ;  // (threads<<32 | smem) -> grid
+  size_t rows_smem = 0;                            // dynamic shared memory a rows CTA may take
+  std::atomic<int> graphs{0};                      // live graphs (the engine outlives them)
   std::string err;
   std::mutex mu;                                   // serialises all GPU work of the engine
 };
@@ -201,10 +222,34 @@ gst_status fail(gst_engine* e, gst_status s, const std::string& msg) {
                   std::string(#call) + ": " + cudaGetErrorString(_e));                \
   } while (0)
 
+// Dynamic shared memory a rows-kernel CTA may take on `device`: the opt-in maximum
+// per block less the kernel's static shared memory.
+size_t rows_smem_limit(int device) {
+  int optin = 0;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess)
+    optin = 48 * 1024;
+  cudaFuncAttributes fa{};
+  cudaFuncGetAttributes(&fa, k_rows);
+  return optin > (int)fa.sharedSizeBytes ? (size_t)optin - fa.sharedSizeBytes : 0;
+}
+
+// Warps per CTA of the rows kernel when the widest resident row has rwm cells: the
+// configured CTA size (threads_per_block, at most 8 warps), fewer when that many
+// warps' rows do not fit the shared memory; 0 when not even one does.
+int rows_warps(size_t smem_limit, int threads_per_block, int rwm) {
+  const size_t per = rows_smem_per_warp(rwm);
+  const int want = std::max(1, std::min(8, threads_per_block / 32));
+  return (int)std::min<size_t>((size_t)want, smem_limit / per);
+}
+
 gst_status validate_query(gst_engine* eng, const gst_groups* grp, const gst_query* q) {
   if (!q || q->k < 1 || q->k > KMAX || !q->group_ids)
     return fail(eng, GST_BAD_INPUT, "query: k must be in [1,8] with group ids");
   if (q->hop_bound > 30) return fail(eng, GST_BAD_INPUT, "query: hop bound must be <= 30");
+  // one row of the query's states must fit one warp's shared memory in the rows kernel
+  // (2^k x (D+1) cells; every k <= 8, D <= 30 row fits the 227 KB of a B200 CTA)
+  if (rows_warps(eng->rows_smem, 32, (int)(((size_t)1 << q->k) * (q->hop_bound >= 0 ? q->hop_bound + 1 : 1))) < 1)
+    return fail(eng, GST_BAD_INPUT, "query: its state row does not fit the rows kernel's shared memory");
   for (int i = 0; i < q->k; i++) {
     const int32_t a = q->group_ids[i];
     if (a < 0 || a >= grp->n) return fail(eng, GST_BAD_INPUT, "query: group id out of range");
@@ -218,7 +263,7 @@ gst_status validate_query(gst_engine* eng, const gst_groups* grp, const gst_quer
 
 gst_status status_of(const Ctx& c) {
   if (c.error & ERR_TIMEOUT) return GST_TIMEOUT;
-  if (c.error & (ERR_QCAP | ERR_FARCAP | ERR_ROWCAP)) return GST_CAPACITY;
+  if (c.error & (ERR_QCAP | ERR_FARCAP | ERR_ROWCAP | ERR_POOL)) return GST_CAPACITY;
   if (c.error) return GST_DEVICE_ERROR;
   if (c.phase != PH_DONE) return GST_DEVICE_ERROR;
   if (c.best == ~0ull) return GST_INFEASIBLE;
@@ -253,6 +298,47 @@ void apply_launch_config(gst_engine* eng) {
   eng->grow_blocks = eng->sms * std::max(1, std::min(occ_grow, eng->cfg.blocks_per_sm));
   eng->sssp_blocks = eng->sms * std::max(1, std::min(occ_sssp, eng->cfg.blocks_per_sm));
   eng->rows_occ.clear();
+}
+
+// The query-dependent fields of a fresh context (zeroed by the caller), shared by the
+// runner's slots and the no-allocation solve: sizes, pruning switches, bounds, phase
+// and the distance search's item form.
+void init_query_ctx(Ctx& c, const gst_query* q, const gst_config& cfg) {
+  const int hop = q->hop_bound >= 0;
+  c.k = q->k;
+  c.W = 1 << q->k;
+  c.full = c.W - 1;
+  c.D = hop ? q->hop_bound : 0;
+  c.DD = hop ? q->hop_bound + 1 : 1;
+  c.RW = c.W * c.DD;
+  c.hop = hop;
+  // The one-label and tour bounds of the unbounded problem are lower bounds of the
+  // hop-bounded one too (a hop-feasible completion is also an unbounded one), so
+  // hop-bounded queries prune with them against their own bound ub_cell.
+  c.use_lb = 1;
+  c.use_tour = 1;
+  c.cut_mult = hop ? (uint32_t)(cfg.hop_cut_mult > 0 ? cfg.hop_cut_mult : 1) : 1u;
+  // A tree of diameter <= D reaches every missing group within D edges of any of its
+  // vertices, so hop-bounded queries bound with the cheapest paths of at most D
+  // edges (a level-synchronous search of D rounds), tighter than unlimited ones.
+  c.sssp_hops = hop && q->hop_bound > 0 ? (uint32_t)q->hop_bound : 0u;
+  for (int i = 0; i < q->k; i++) c.gid[i] = q->group_ids[i];
+  memset(c.vv, 0xFF, sizeof(c.vv));
+  c.delta = (uint32_t)std::max(0, cfg.bucket_delta);
+  c.max_levels = (uint32_t)cfg.max_levels;
+  c.in_idx = 1;
+  c.far_min = 0xFFFFFFFFu;
+  // the hop-limited search runs one round per step, in one cost bucket
+  c.bucket_end = c.delta && !c.sssp_hops ? c.delta : 0xFFFFFFFFu;
+  c.ub = 0xFFFFFFFFu;
+  c.cut = 0xFFFFFFFFu;
+  c.ub_cell = 0xFFFFFFFFu;
+  c.ub_hop = 0xFFFFFFFFu;
+  c.best = ~0ull;
+  c.phase = c.use_lb ? PH_SSSP : PH_DP;
+  // one distance-search item per (vertex, groups): hop-limited distances in rounds,
+  // unlimited ones when the search runs in one bucket
+  c.sssp_mask = c.sssp_hops ? 2u : (c.bucket_end == 0xFFFFFFFFu ? 1u : 0u);
 }
 
 enum ProfKind { PROF_GROW = 0, PROF_ROWS = 1, PROF_SSSP = 2 };
@@ -372,13 +458,14 @@ struct Runner {
     SlotMem tmp;
     const int split = eng->cfg.split_degree;
     const uint32_t cap = list_cap(g->V, g->E, j.rw, split, j.boost);
-    return carve_slot(tmp, nullptr, g->V, j.rw, cap, eng->cfg.bucket_delta > 0 ? cap : 0, j.nhb);
+    return carve_slot(tmp, nullptr, g->V, j.rw, pool_rows(g->V, j.boost), cap,
+                      eng->cfg.bucket_delta > 0 ? cap : 0, j.nhb);
   }
 
   int rw_max() const {
     size_t r = 1;
     for (int s = 0; s < nctx; s++)
-      if (owner[s]) r = std::max(r, mem[s].rw);
+      if (owner[s]) r = std::max(r, owner[s]->rw);
     return (int)r;
   }
 
@@ -458,15 +545,24 @@ struct Runner {
     }
     if (!*out) {
       // hand wholly free arenas back to the pool while a new one would not fit
+      bool freed = false;
       for (size_t i = 0; i < arenas.size() && held + need > budget;) {
         Arena& a = arenas[i];
         if (a.free_.size() == 1 && a.free_[0].first == 0 && a.free_[0].second == a.size) {
           cudaFreeAsync(a.base, eng->stream);
           held -= a.size;
           arenas.erase(arenas.begin() + (long)i);
+          freed = true;
         } else {
           i++;
         }
+      }
+      if (freed) {
+        // the pool keeps freed memory reserved (its release threshold is unlimited):
+        // give it back to the device before a new arena is mapped, or the pool would
+        // hold both and run the device out of memory within the budget
+        CK(cudaStreamSynchronize(eng->stream));
+        CK(cudaMemPoolTrimTo(eng->pool, held));
       }
       bool grown = false;
       gst_status st = arena_grow(need, &grown);
@@ -485,12 +581,13 @@ struct Runner {
     const uint32_t farcap = eng->cfg.bucket_delta > 0 ? cap : 0;
     const size_t need = job_bytes(*j);
     if (need > budget) return GST_OOM_ADMISSION;
+    const size_t need_table = (size_t)pool_rows(g->V, j->boost) * j->rw * 8;
     // the free slot whose memory already fits with the least to spare (a small query
     // does not take a large slot that a large one will want; among equals the lowest,
     // which keeps the contexts the kernels scan few), else the lowest free slot
     int s = -1;
     for (int i = 0; i < max_slots; i++)
-      if (!owner[i] && mem[i].base && mem[i].rw >= j->rw && mem[i].cap >= cap &&
+      if (!owner[i] && mem[i].base && mem[i].table_bytes >= need_table && mem[i].cap >= cap &&
           mem[i].farcap >= farcap && mem[i].nhb >= j->nhb && (s < 0 || mem[i].bytes < mem[s].bytes))
         s = i;
     if (s < 0) {
@@ -506,7 +603,7 @@ struct Runner {
       if (st != GST_OK) return st;
       if (!p) return GST_NOT_READY;
       SlotMem m;
-      carve_slot(m, (unsigned char*)p, g->V, j->rw, cap, farcap, j->nhb);
+      carve_slot(m, (unsigned char*)p, g->V, j->rw, pool_rows(g->V, j->boost), cap, farcap, j->nhb);
       m.base = p;
       m.bytes = need;
       mem[s] = m;
@@ -518,6 +615,7 @@ struct Runner {
     const gst_query* q = &j->q;
     const int hop = q->hop_bound >= 0;
     c.table = m.table;
+    c.rowmap = m.rowmap;
     c.dist = m.dist;
     c.rowbits = m.rowbits;
     c.fm[0] = m.fm[0];
@@ -538,39 +636,7 @@ struct Runner {
     c.rowcap = m.rowcap;
     c.outcap = m.outcap;
     c.stackcap = m.stackcap;
-    c.k = q->k;
-    c.W = 1 << q->k;
-    c.full = c.W - 1;
-    c.D = hop ? q->hop_bound : 0;
-    c.DD = hop ? q->hop_bound + 1 : 1;
-    c.RW = c.W * c.DD;
-    c.hop = hop;
-    // The one-label and tour bounds of the unbounded problem are lower bounds of the
-    // hop-bounded one too (a hop-feasible completion is also an unbounded one), so
-    // hop-bounded queries prune with them against their own bound ub_cell.
-    c.use_lb = 1;
-    c.use_tour = 1;
-    c.cut_mult = hop ? (uint32_t)(eng->cfg.hop_cut_mult > 0 ? eng->cfg.hop_cut_mult : 1) : 1u;
-    // A tree of diameter <= D reaches every missing group within D edges of any of its
-    // vertices, so hop-bounded queries bound with the cheapest paths of at most D
-    // edges (a level-synchronous search of D rounds), tighter than unlimited ones.
-    c.sssp_hops = hop && q->hop_bound > 0 ? (uint32_t)q->hop_bound : 0u;
-    for (int i = 0; i < q->k; i++) c.gid[i] = q->group_ids[i];
-    memset(c.vv, 0xFF, sizeof(c.vv));
-    c.delta = (uint32_t)std::max(0, eng->cfg.bucket_delta);
-    c.max_levels = (uint32_t)eng->cfg.max_levels;
-    c.in_idx = 1;
-    c.far_min = 0xFFFFFFFFu;
-    // the hop-limited search runs one round per step, in one cost bucket
-    c.bucket_end = c.delta && !c.sssp_hops ? c.delta : 0xFFFFFFFFu;
-    // one distance-search item per (vertex, groups): hop-limited distances in rounds,
-    // unlimited ones when the search runs in one bucket
-    c.ub = 0xFFFFFFFFu;
-    c.cut = 0xFFFFFFFFu;
-    c.ub_cell = 0xFFFFFFFFu;
-    c.ub_hop = 0xFFFFFFFFu;
-    c.best = ~0ull;
-    c.phase = c.use_lb ? PH_SSSP : PH_DP;
+    init_query_ctx(c, q, eng->cfg);
     // a group-cache fill: the distances of one group, exact everywhere, then done
     if (j->cache_dst) {
       c.dist_only = 1;
@@ -605,13 +671,18 @@ struct Runner {
     }
     c.sssp_mask = c.sssp_hops ? 2u : (c.bucket_end == 0xFFFFFFFFu ? 1u : 0u);
     cudaStream_t st = eng->stream;
-    CK(cudaMemsetAsync(m.table, 0xFF, (size_t)g->V * (size_t)c.RW * 8, st));
+    // the pool takes every row the slot's table holds; only the rows the slot's last
+    // query wrote need clearing
+    c.pool_cap = (uint32_t)std::min<uint64_t>((uint64_t)g->V, m.table_bytes / ((size_t)c.RW * 8));
+    c.pool_n = 0;
+    if (c.pool_cap >= (uint32_t)g->V) c.rowmap = nullptr;  // a row for every vertex: dense
+    if (m.table_dirty) CK(cudaMemsetAsync(m.table, 0xFF, m.table_dirty, st));
+    m.table_dirty = 0;
+    if (c.rowmap) CK(cudaMemsetAsync(m.rowmap, 0xFF, (size_t)g->V * 4, st));
     CK(cudaMemsetAsync(m.rowbits, 0, ((size_t)g->V + 31) / 32 * 4, st));
     if (c.use_lb && !cached) CK(cudaMemsetAsync(m.dist, 0xFF, (size_t)g->V * DIST_STRIDE * 4, st));
-    if (c.sssp_mask) {
-      CK(cudaMemsetAsync(m.fm[0], 0, ((size_t)g->V + 3) / 4 * 4, st));
-      CK(cudaMemsetAsync(m.fm[1], 0, ((size_t)g->V + 3) / 4 * 4, st));
-    }
+    CK(cudaMemsetAsync(m.fm[0], 0, fm_bytes(g->V), st));
+    CK(cudaMemsetAsync(m.fm[1], 0, fm_bytes(g->V), st));
     if (c.nhb && !cached)
       CK(cudaMemsetAsync(m.dist_h, 0xFF, (size_t)c.nhb * (size_t)g->V * DIST_STRIDE * 4, st));
     CK(cudaMemcpyAsync(d_ctx + s, &c, sizeof(Ctx), cudaMemcpyHostToDevice, st));
@@ -690,7 +761,8 @@ struct Runner {
       k_ctrl<<<nctx, 128, 0, st>>>(d_ctx, nctx, CTRL_SSSP);
     }
     const size_t per_warp = rows_smem_per_warp(rwm);
-    const int warps = std::max(2, std::min(8, tpb / 32));  // k_rows: at most 256 threads
+    // k_rows: at most 256 threads, as many warps as the widest row lets fit
+    const int warps = rows_warps(eng->rows_smem, tpb, rwm);
     int pe = prof ? prof_begin(PROF_ROWS) : -1;
     k_rows<<<rows_blocks(eng, warps * 32, per_warp * warps), warps * 32, per_warp * warps, st>>>(
         d_ctx, nctx, G, split, rwm);
@@ -726,7 +798,7 @@ struct Runner {
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     {
       // occupancy queries before the capture
-      const int warps = std::max(2, std::min(8, eng->cfg.threads_per_block / 32));
+      const int warps = rows_warps(eng->rows_smem, eng->cfg.threads_per_block, rwm);
       rows_blocks(eng, warps * 32, rows_smem_per_warp(rwm) * warps);
     }
     cudaStream_t cap;
@@ -828,8 +900,14 @@ struct Runner {
       const Ctx c = h_ctx[s];
       owner[s] = nullptr;
       active--;
-      if ((c.error & (ERR_QCAP | ERR_FARCAP)) &&
-          !cap_is_worst(g->V, g->E, j->rw, eng->cfg.split_degree, c.qcap)) {
+      // pool rows this query may have written: cleared before the slot's next query
+      mem[s].table_dirty = std::max(mem[s].table_dirty,
+                                    (size_t)(c.rowmap ? std::min(c.pool_n, c.pool_cap) : c.pool_cap) *
+                                        (size_t)c.RW * 8);
+      const bool list_full = (c.error & (ERR_QCAP | ERR_FARCAP)) &&
+                             !cap_is_worst(g->V, g->E, j->rw, eng->cfg.split_degree, c.qcap);
+      const bool pool_full = (c.error & ERR_POOL) && c.rowmap != nullptr;
+      if (list_full || pool_full) {
         j->boost++;
         retry.push_back(j);
         continue;
@@ -1121,13 +1199,22 @@ gst_status gst_engine_create(int32_t device, const gst_config* cfg, gst_engine**
   }
   uint64_t keep = ~0ull;
   cudaMemPoolSetAttribute(eng->pool, cudaMemPoolAttrReleaseThreshold, &keep);
-  cudaFuncSetAttribute(k_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  eng->rows_smem = rows_smem_limit(device);
+  if (cudaFuncSetAttribute(k_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)eng->rows_smem) != cudaSuccess) {
+    cudaStreamDestroy(eng->stream);
+    cudaMemPoolDestroy(eng->pool);
+    delete eng;
+    return fail(nullptr, GST_DEVICE_ERROR, "engine: cannot size the rows kernel's shared memory");
+  }
   *out = eng;
   return GST_OK;
 }
 
 gst_status gst_engine_destroy(gst_engine* eng) {
   if (!eng) return GST_OK;
+  if (eng->graphs.load() > 0)
+    return fail(eng, GST_BAD_INPUT, "engine: destroy its graphs first (gst_graph_destroy)");
   cudaSetDevice(eng->device);
   if (eng->stream) {
     cudaStreamSynchronize(eng->stream);
@@ -1222,6 +1309,7 @@ static gst_status graph_create_impl(gst_engine* eng, int64_t V, int64_t E, const
   CK(cudaMemcpyAsync(g->d_widx, widx.data(), sizeof(uint32_t) * V * WIDX,
                      cudaMemcpyHostToDevice, eng->stream));
   CK(cudaStreamSynchronize(eng->stream));
+  eng->graphs++;
   *out = g;
   return GST_OK;
 }
@@ -1258,6 +1346,7 @@ gst_status gst_graph_destroy(gst_graph* g) {
   cudaFree(g->d_widx);
   cudaMemPoolTrimTo(eng->pool, 0);
   delete g;
+  eng->graphs--;
   return GST_OK;
 }
 
@@ -1586,7 +1675,7 @@ gst_status gst_debug_slot_state(gst_graph* g, int32_t slot, uint64_t* cells, int
   CK(cudaSetDevice(eng->device));
   Runner& R = *g->batch;
   const SlotMem& m = R.mem[slot];
-  const int64_t have = (int64_t)(g->V * (int64_t)m.rw);
+  const int64_t have = (int64_t)(m.table_bytes / 8);
   if (cells && n_cells)
     CK(cudaMemcpyAsync(cells, m.table, (size_t)std::min(n_cells, have) * 8,
                        cudaMemcpyDeviceToHost, eng->stream));
@@ -1895,39 +1984,67 @@ constexpr size_t kNoallocScratchBytes = (size_t)64 << 20;  // GST_NOALLOC_SCRATC
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratchBytes];
 
 constexpr int kMaxDevices = 64;
+constexpr uint32_t kNoallocOutCap = 1u << 14;    // tree edges the extraction may write
+constexpr uint32_t kNoallocStackCap = 1u << 16;  // its parent-walk stack
+
+// Per-device set-up, done once with the device current: the scratch array's device
+// address, the rows kernel's shared-memory limit and two timing events.
+struct NoallocDev {
+  bool ready = false;
+  void* scratch = nullptr;
+  size_t rows_smem = 0;
+  int sms = 0, grow_blocks = 0, sssp_blocks = 0;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+};
 std::mutex g_noalloc_mu;
-void* g_noalloc_ptr[kMaxDevices] = {nullptr};
+NoallocDev g_noalloc_dev[kMaxDevices];
+// Host staging of the raw extracted edges (u, v, w), sorted and deduplicated here before
+// they are copied into the caller's arrays; shared by all calls (under g_noalloc_mu).
+int32_t g_noalloc_edges[3 * kNoallocOutCap];
 
-
-// Device address of the scratch array on `device` (must be current).  Host code
-// cannot use the symbol itself: on the host it names a stand-in object, not
-// device memory.
-gst_status noalloc_scratch(int device, void** out) {
-  std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_ptr[device]) {
+// Device address of the scratch array (and the rest of the set-up) on `device`, which
+// must be current.  Host code cannot use the symbol itself: on the host it names a
+// stand-in object, not device memory.
+gst_status noalloc_setup(int device, NoallocDev** out, std::string* err) {
+  NoallocDev& d = g_noalloc_dev[device];
+  if (!d.ready) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) {
-      tl_err = std::string("noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e);
+      *err = std::string("noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e);
       return GST_DEVICE_ERROR;
     }
-    g_noalloc_ptr[device] = p;
+    d.scratch = p;
+    d.rows_smem = rows_smem_limit(device);
+    e = cudaFuncSetAttribute(k_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.rows_smem);
+    int occ_grow = 1, occ_sssp = 1;
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_grow, k_grow, 256, 0);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sssp, k_sssp, 256, 0);
+    if (e == cudaSuccess) e = cudaEventCreate(&d.ev[0]);
+    if (e == cudaSuccess) e = cudaEventCreate(&d.ev[1]);
+    if (e != cudaSuccess) {
+      *err = std::string("noalloc: device set-up: ") + cudaGetErrorString(e);
+      return GST_DEVICE_ERROR;
+    }
+    gst_config cfg;
+    gst_config_default(&cfg);
+    d.grow_blocks = d.sms * std::max(1, std::min(occ_grow, cfg.blocks_per_sm));
+    d.sssp_blocks = d.sms * std::max(1, std::min(occ_sssp, cfg.blocks_per_sm));
+    d.ready = true;
   }
-  *out = g_noalloc_ptr[device];
+  *out = &d;
   return GST_OK;
-}
-
-gst_status noalloc_fail(gst_status s, const char* msg) {
-  tl_err = msg;
-  return s;
 }
 
 gst_status noalloc_solve(int device, cudaStream_t st, int64_t V, int64_t E, const int64_t* d_beg,
                          const int32_t* d_edges, int32_t n_groups, const int64_t* d_grp_ptr,
                          const int32_t* d_members, const gst_query* q, int64_t edge_cap,
                          gst_result* res) {
-  gst_engine* eng = nullptr;  // for CK()
-  if (!res) return noalloc_fail(GST_BAD_INPUT, "noalloc: null result");
+  if (!res) {
+    tl_err = "noalloc: null result";
+    return GST_BAD_INPUT;
+  }
   int32_t* eu = res->edge_u;
   int32_t* ev = res->edge_v;
   int32_t* ew = res->edge_w;
@@ -1935,88 +2052,108 @@ gst_status noalloc_solve(int device, cudaStream_t st, int64_t V, int64_t E, cons
   res->edge_u = eu;
   res->edge_v = ev;
   res->edge_w = ew;
+  // every failure leaves its status in res->status as well as in the return value
+  auto failed = [&](gst_status s, const std::string& msg) {
+    res->status = s;
+    tl_err = msg;
+    return s;
+  };
   if (!q || !d_beg || !d_grp_ptr || !d_members || (E > 0 && !d_edges) || V < 1 ||
       V >= ((int64_t)1 << 27) || E < 0 || n_groups < 1 || edge_cap < 0 ||
       (edge_cap > 0 && (!eu || !ev || !ew)))
-    return noalloc_fail(GST_BAD_INPUT, "noalloc: bad arguments");
+    return failed(GST_BAD_INPUT, "noalloc: bad arguments");
   res->user_tag = q->user_tag;
   if (q->k < 1 || q->k > KMAX || !q->group_ids || q->hop_bound > 30)
-    return res->status = GST_BAD_INPUT,
-           noalloc_fail(GST_BAD_INPUT, "noalloc: k must be in [1,8], hop bound <= 30");
+    return failed(GST_BAD_INPUT, "noalloc: k must be in [1,8], hop bound <= 30");
   for (int i = 0; i < q->k; i++) {
     const int32_t a = q->group_ids[i];
-    if (a < 0 || a >= n_groups)
-      return res->status = GST_BAD_INPUT, noalloc_fail(GST_BAD_INPUT, "noalloc: group id out of range");
+    if (a < 0 || a >= n_groups) return failed(GST_BAD_INPUT, "noalloc: group id out of range");
     for (int j = 0; j < i; j++)
-      if (q->group_ids[j] == a)
-        return res->status = GST_BAD_INPUT, noalloc_fail(GST_BAD_INPUT, "noalloc: duplicate group id");
+      if (q->group_ids[j] == a) return failed(GST_BAD_INPUT, "noalloc: duplicate group id");
   }
-  // scratch layout; reject what does not fit
-  const int hop = q->hop_bound >= 0;
-  const size_t RW = row_width(q->k, q->hop_bound);
-  const uint32_t outcap = 1u << 14, stackcap = 1u << 16;
+  // scratch layout (the same buffers as a runner slot); reject what does not fit
+  gst_config cfg;
+  gst_config_default(&cfg);
+  Ctx c;
+  memset(&c, 0, sizeof(c));
+  init_query_ctx(c, q, cfg);
+  const size_t RW = (size_t)c.RW;
+  const int nhb = c.sssp_hops ? hop_budgets(q->hop_bound) : 0;
+  const size_t Vs = (size_t)V;
   size_t off = align256(sizeof(Ctx));
-  const size_t o_table = off;
-  off = align256(off + (size_t)V * RW * 8);
-  const size_t o_dist = off;
-  off = align256(off + (size_t)V * DIST_STRIDE * 4);
-  const size_t o_bits = off;
-  off = align256(off + ((size_t)V + 31) / 32 * 4);
-  const size_t o_rows = off;
-  off = align256(off + (size_t)V * 4);
-  const size_t o_out = off;
-  off = align256(off + (size_t)outcap * 12);
-  const size_t o_stack = off;
-  off = align256(off + (size_t)stackcap * 8);
-  const size_t o_tour = off;
-  off = align256(off + kTourWords * 4);
-  const size_t min_lists = 4 * (size_t)(4 * V + 4096) * 16;
+  auto take = [&](size_t n) {
+    const size_t o = off;
+    off = align256(off + n);
+    return o;
+  };
+  const size_t o_table = take(Vs * RW * 8);
+  const size_t o_dist = take(Vs * DIST_STRIDE * 4);
+  const size_t o_bits = take((Vs + 31) / 32 * 4);
+  const size_t o_rows = take(Vs * 4);
+  const size_t o_out = take((size_t)kNoallocOutCap * 12);
+  const size_t o_stack = take((size_t)kNoallocStackCap * 8);
+  const size_t o_tour = take(kTourWords * 4);
+  const size_t o_fm0 = take(fm_bytes(V));
+  const size_t o_fm1 = take(fm_bytes(V));
+  const size_t o_snap = take(c.sssp_mask == 2u ? Vs * DIST_STRIDE * 4 : 0);
+  const size_t o_dh = take((size_t)nhb * Vs * DIST_STRIDE * 4);
+  // four worklists (near and far, ping-pong) of at least 4V + 4096 items each
+  const size_t min_lists = 4 * (4 * Vs + 4096) * 16;
   if (off + min_lists > kNoallocScratchBytes) {
     char msg[200];
     snprintf(msg, sizeof msg,
              "noalloc: this query needs more than the %zu-byte static scratch "
              "(V=%lld, row width %zu); use gst_solve",
              kNoallocScratchBytes, (long long)V, RW);
-    res->status = GST_OOM_ADMISSION;
-    return noalloc_fail(GST_OOM_ADMISSION, msg);
+    return failed(GST_OOM_ADMISSION, msg);
   }
   const uint64_t want = (uint64_t)V * RW + 4ull * (uint64_t)V + 4096;
   const uint64_t fit = (kNoallocScratchBytes - off) / (4 * 16);
   const uint32_t cap = (uint32_t)std::min<uint64_t>(std::min<uint64_t>(want, fit), 1ull << 26);
 
+  // the caller's device stays current for the caller: switch, and switch back on every exit
   int prev_dev = 0;
-  CK(cudaGetDevice(&prev_dev));
-  CK(cudaSetDevice(device));
-  void* scratch = nullptr;
-  gst_status s = noalloc_scratch(device, &scratch);
-  if (s != GST_OK) {
-    cudaSetDevice(prev_dev);
-    res->status = s;
-    return s;
+  if (cudaGetDevice(&prev_dev) != cudaSuccess) return failed(GST_DEVICE_ERROR, "noalloc: cudaGetDevice failed");
+  if (cudaSetDevice(device) != cudaSuccess) return failed(GST_DEVICE_ERROR, "noalloc: cudaSetDevice failed");
+  struct RestoreDevice {
+    int dev;
+    ~RestoreDevice() { cudaSetDevice(dev); }
+  } restore{prev_dev};
+#define NCK(call)                                                                         \
+  do {                                                                                    \
+    cudaError_t _e = (call);                                                              \
+    if (_e != cudaSuccess)                                                                \
+      return failed(GST_DEVICE_ERROR, std::string(#call) + ": " + cudaGetErrorString(_e)); \
+  } while (0)
+
+  // one call at a time per process: the scratch, the set-up and the host staging are shared
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  NoallocDev* nd = nullptr;
+  {
+    std::string err;
+    gst_status s = noalloc_setup(device, &nd, &err);
+    if (s != GST_OK) return failed(s, err);
   }
-  unsigned char* base = (unsigned char*)scratch;
+  const int warps = rows_warps(nd->rows_smem, cfg.threads_per_block, (int)RW);
+  if (warps < 1) return failed(GST_BAD_INPUT, "noalloc: the query's state row does not fit the rows kernel's shared memory");
+  unsigned char* base = (unsigned char*)nd->scratch;
   // empty-group check: members of each queried group
   for (int i = 0; i < q->k; i++) {
     int64_t be[2];
-    CK(cudaMemcpyAsync(be, d_grp_ptr + q->group_ids[i], sizeof(be), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    if (be[1] <= be[0]) {
-      cudaSetDevice(prev_dev);
-      res->status = GST_BAD_INPUT;
-      return noalloc_fail(GST_BAD_INPUT, "noalloc: group has no members");
-    }
+    NCK(cudaMemcpyAsync(be, d_grp_ptr + q->group_ids[i], sizeof(be), cudaMemcpyDeviceToHost, st));
+    NCK(cudaStreamSynchronize(st));
+    if (be[1] <= be[0]) return failed(GST_BAD_INPUT, "noalloc: group has no members");
   }
-  int sms = 148;
-  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-  gst_config cfg;
-  gst_config_default(&cfg);
   const int split = cfg.split_degree;
-  Ctx c;
-  memset(&c, 0, sizeof(c));
   c.table = (uint64_t*)(base + o_table);
   c.dist = (uint32_t*)(base + o_dist);
   c.rowbits = (uint32_t*)(base + o_bits);
   c.tour = (uint32_t*)(base + o_tour);
+  c.fm[0] = (uint32_t*)(base + o_fm0);
+  c.fm[1] = (uint32_t*)(base + o_fm1);
+  c.snap = (uint32_t*)(base + o_snap);
+  c.dist_h = (uint32_t*)(base + o_dh);
+  c.nhb = nhb;
   c.q[0] = (uint4*)(base + off);
   c.q[1] = (uint4*)(base + off + (size_t)cap * 16);
   c.far[0] = (uint4*)(base + off + 2 * (size_t)cap * 16);
@@ -2026,116 +2163,103 @@ gst_status noalloc_solve(int device, cudaStream_t st, int64_t V, int64_t E, cons
   c.stack = (uint64_t*)(base + o_stack);
   c.qcap = c.farcap = cap;
   c.rowcap = (uint32_t)V;
-  c.outcap = outcap;
-  c.stackcap = stackcap;
-  c.k = q->k;
-  c.W = 1 << q->k;
-  c.full = c.W - 1;
-  c.D = hop ? q->hop_bound : 0;
-  c.DD = hop ? q->hop_bound + 1 : 1;
-  c.RW = c.W * c.DD;
-  c.hop = hop;
-  c.use_lb = hop ? 0 : 1;
-  c.use_tour = c.use_lb;
-  for (int i = 0; i < q->k; i++) c.gid[i] = q->group_ids[i];
-  memset(c.vv, 0xFF, sizeof(c.vv));
-  c.delta = 0;
-  c.max_levels = (uint32_t)cfg.max_levels;
-  c.in_idx = 1;
-  c.far_min = 0xFFFFFFFFu;
-  c.bucket_end = 0xFFFFFFFFu;
-  c.ub = 0xFFFFFFFFu;
-  c.cut = 0xFFFFFFFFu;
-  c.ub_cell = 0xFFFFFFFFu;
-  c.ub_hop = 0xFFFFFFFFu;
-  c.best = ~0ull;
-  c.phase = c.use_lb ? PH_SSSP : PH_DP;
+  c.outcap = kNoallocOutCap;
+  c.stackcap = kNoallocStackCap;
   Ctx* d_ctx = (Ctx*)base;
-  // clear what must start empty, then upload the context
-  CK(cudaMemsetAsync(c.table, 0xFF, (size_t)V * RW * 8, st));
-  CK(cudaMemsetAsync(c.dist, 0xFF, (size_t)V * DIST_STRIDE * 4, st));
-  CK(cudaMemsetAsync(c.rowbits, 0, ((size_t)V + 31) / 32 * 4, st));
-  CK(cudaMemcpyAsync(d_ctx, &c, sizeof(Ctx), cudaMemcpyHostToDevice, st));
+  NCK(cudaEventRecord(nd->ev[0], st));
+  // clear what must start empty (the array keeps the previous call's contents), then
+  // upload the context
+  NCK(cudaMemsetAsync(c.table, 0xFF, Vs * RW * 8, st));
+  NCK(cudaMemsetAsync(c.dist, 0xFF, Vs * DIST_STRIDE * 4, st));
+  NCK(cudaMemsetAsync(c.rowbits, 0, (Vs + 31) / 32 * 4, st));
+  NCK(cudaMemsetAsync(c.fm[0], 0, fm_bytes(V), st));
+  NCK(cudaMemsetAsync(c.fm[1], 0, fm_bytes(V), st));
+  if (nhb) NCK(cudaMemsetAsync(c.dist_h, 0xFF, (size_t)nhb * Vs * DIST_STRIDE * 4, st));
+  NCK(cudaMemcpyAsync(d_ctx, &c, sizeof(Ctx), cudaMemcpyHostToDevice, st));
   // the caller's edges are sorted by neighbour only: no light-edge index
   DevGraph G{V, E, d_beg, (const int2*)d_edges, (const int2*)d_edges, nullptr};
   k_init<<<dim3(64, 1), 256, 0, st>>>(d_ctx, 1, G, d_grp_ptr, d_members, split);
   k_ctrl<<<1, 32, 0, st>>>(d_ctx, 1, CTRL_SSSP);
-  const int blocks = sms * cfg.blocks_per_sm;
-  const size_t per_warp = rows_smem_per_warp((int)RW);
-  const int warps = cfg.threads_per_block / 32;
-  cudaFuncSetAttribute(k_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  const size_t smem = rows_smem_per_warp((int)RW) * (size_t)warps;
   int64_t launches = 2;
   Ctx h;
-  const auto t0 = std::chrono::steady_clock::now();
   for (;;) {
     for (int i = 0; i < 6; i++) {
-      k_sssp<<<blocks, 256, 0, st>>>(d_ctx, 1, G, split);
-      k_ctrl<<<1, 32, 0, st>>>(d_ctx, 1, CTRL_SSSP);
-      k_rows<<<blocks, warps * 32, per_warp * warps, st>>>(d_ctx, 1, G, split, (int)RW);
-      k_ctrl<<<1, 32, 0, st>>>(d_ctx, 1, CTRL_DP_ROWS);
-      k_grow<<<blocks, 256, 0, st>>>(d_ctx, 1, G, split);
-      k_ctrl<<<1, 32, 0, st>>>(d_ctx, 1, CTRL_DP_GROW);
+      k_sssp<<<nd->sssp_blocks, 256, 0, st>>>(d_ctx, 1, G, split);
+      k_ctrl<<<1, 128, 0, st>>>(d_ctx, 1, CTRL_SSSP);
+      k_rows<<<nd->sms * 4, warps * 32, smem, st>>>(d_ctx, 1, G, split, (int)RW);
+      k_ctrl<<<1, 128, 0, st>>>(d_ctx, 1, CTRL_DP_ROWS);
+      k_grow<<<nd->grow_blocks, 256, 0, st>>>(d_ctx, 1, G, split);
+      k_ctrl<<<1, 128, 0, st>>>(d_ctx, 1, CTRL_DP_GROW);
       launches += 6;
     }
-    CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(&h, d_ctx, sizeof(Ctx), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
+    NCK(cudaGetLastError());
+    NCK(cudaMemcpyAsync(&h, d_ctx, sizeof(Ctx), cudaMemcpyDeviceToHost, st));
+    NCK(cudaStreamSynchronize(st));
     if (h.phase >= PH_DONE) break;
   }
   k_extract<<<1, 32, 0, st>>>(d_ctx, 1, G);
   launches++;
-  CK(cudaMemcpyAsync(&h, d_ctx, sizeof(Ctx), cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
-  res->status = status_of(h);
-  if (h.error & ERR_EXTRACT) res->status = GST_DEVICE_ERROR;
+  NCK(cudaGetLastError());
+  NCK(cudaEventRecord(nd->ev[1], st));
+  NCK(cudaMemcpyAsync(&h, d_ctx, sizeof(Ctx), cudaMemcpyDeviceToHost, st));
+  const uint32_t nraw = std::min(h.n_out, kNoallocOutCap);
+  if (status_of(h) == GST_OK && !(h.error & ERR_EXTRACT) && nraw > 0)
+    NCK(cudaMemcpyAsync(g_noalloc_edges, c.out, (size_t)nraw * 12, cudaMemcpyDeviceToHost, st));
+  NCK(cudaStreamSynchronize(st));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, nd->ev[0], nd->ev[1]);
+  gst_status status = status_of(h);
+  if (h.error & ERR_EXTRACT) status = GST_DEVICE_ERROR;
   res->stats.levels = h.levels;
   res->stats.states_expanded = (int64_t)h.st_items;
   res->stats.edge_relaxations = (int64_t)h.st_relax;
   res->stats.merge_pairs = (int64_t)h.st_merge;
   res->stats.rows_merged = (int64_t)h.st_rows;
   res->stats.sssp_relaxations = (int64_t)h.st_sssp;
+  res->stats.queue_max = h.st_qmax;
   res->stats.kernel_launches = launches;
-  res->stats.latency_ms =
-      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-  res->stats.device_ms = res->stats.latency_ms;
-  if (res->status == GST_OK) {
-    res->cost = (int32_t)(h.best >> 32);
-    res->root = (int32_t)(h.best & 0x7FFFFFFull);
-    res->root_hop = (int32_t)((h.best >> 27) & 31u);
-    const int64_t nraw = std::min<int64_t>(h.n_out, outcap);
-    if (nraw > edge_cap) {
-      res->status = GST_CAPACITY;
-    } else if (nraw > 0) {
-      // scatter the interleaved (u, v, w) triples into the caller's three arrays
-      CK(cudaMemcpy2DAsync(eu, 4, c.out + 0, 12, 4, (size_t)nraw, cudaMemcpyDeviceToHost, st));
-      CK(cudaMemcpy2DAsync(ev, 4, c.out + 1, 12, 4, (size_t)nraw, cudaMemcpyDeviceToHost, st));
-      CK(cudaMemcpy2DAsync(ew, 4, c.out + 2, 12, 4, (size_t)nraw, cudaMemcpyDeviceToHost, st));
-      CK(cudaStreamSynchronize(st));
-      // in place: orient u < v, drop repeated edges, sort by (u, v)
-      int64_t m = 0;
-      for (int64_t i = 0; i < nraw; i++) {
-        int32_t a = eu[i], b = ev[i];
-        if (a > b) std::swap(a, b);
-        bool dup = false;
-        for (int64_t j = 0; j < m && !dup; j++) dup = eu[j] == a && ev[j] == b;
-        if (dup) continue;
-        const int32_t w = ew[i];
-        int64_t p = m++;
-        while (p > 0 && (eu[p - 1] > a || (eu[p - 1] == a && ev[p - 1] > b))) {
-          eu[p] = eu[p - 1];
-          ev[p] = ev[p - 1];
-          ew[p] = ew[p - 1];
-          p--;
-        }
-        eu[p] = a;
-        ev[p] = b;
-        ew[p] = w;
-      }
-      res->n_edges = m;
+  res->stats.device_ms = ms;
+  res->stats.h2d_bytes = (int64_t)sizeof(Ctx);
+  res->stats.d2h_bytes = 2 * (int64_t)sizeof(Ctx) + (int64_t)nraw * 12 + 16 * q->k;
+  if (status != GST_OK) {
+    if (status == GST_INFEASIBLE) {
+      res->status = status;
+      return status;
     }
+    char msg[160];
+    snprintf(msg, sizeof msg, "noalloc: phase %u error bits 0x%x levels %u", h.phase, h.error, h.levels);
+    return failed(status, msg);
   }
-  cudaSetDevice(prev_dev);
-  return res->status == GST_OK ? GST_OK : (gst_status)res->status;
+  res->cost = (int32_t)(h.best >> 32);
+  res->root = (int32_t)(h.best & 0x7FFFFFFull);
+  res->root_hop = (int32_t)((h.best >> 27) & 31u);
+  // orient each edge u < v, sort by (u, v) and drop repeats (the parent walk reaches
+  // an edge once per state that uses it), then copy into the caller's arrays
+  struct Tri {
+    int32_t u, v, w;
+  };
+  Tri* t = (Tri*)g_noalloc_edges;
+  for (uint32_t i = 0; i < nraw; i++)
+    if (t[i].u > t[i].v) std::swap(t[i].u, t[i].v);
+  std::sort(t, t + nraw, [](const Tri& a, const Tri& b) { return a.u != b.u ? a.u < b.u : a.v < b.v; });
+  Tri* end = std::unique(t, t + nraw, [](const Tri& a, const Tri& b) { return a.u == b.u && a.v == b.v; });
+  const int64_t m = end - t;
+  if (m > edge_cap) {
+    char msg[160];
+    snprintf(msg, sizeof msg, "noalloc: the tree has %lld edges, more than edge_cap = %lld",
+             (long long)m, (long long)edge_cap);
+    return failed(GST_CAPACITY, msg);
+  }
+  for (int64_t i = 0; i < m; i++) {
+    eu[i] = t[i].u;
+    ev[i] = t[i].v;
+    ew[i] = t[i].w;
+  }
+  res->n_edges = m;
+  res->status = GST_OK;
+  return GST_OK;
+#undef NCK
 }
 
 }  // namespace
@@ -2147,8 +2271,11 @@ extern "C" gst_status gst_solve_noalloc(int32_t device, void* stream, int64_t V,
                                         int64_t edge_cap, gst_result* res) {
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev ||
-      device >= kMaxDevices)
-    return noalloc_fail(GST_BAD_INPUT, "noalloc: bad device");
+      device >= kMaxDevices) {
+    tl_err = "noalloc: bad device";
+    if (res) res->status = GST_BAD_INPUT;
+    return GST_BAD_INPUT;
+  }
   return noalloc_solve(device, (cudaStream_t)stream, V, E, d_beg_pos, d_edges, n_groups,
                        d_grp_ptr, d_members, q, edge_cap, res);
 }

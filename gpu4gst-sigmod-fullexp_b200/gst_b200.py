@@ -16,6 +16,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import weakref
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -381,6 +382,7 @@ class Engine:
 
     def __init__(self, device: int = 0, config: Config | None = None, **kw):
         self._h = _vp()
+        self._graphs = weakref.WeakSet()  # closed before the engine
         cfg = config if config is not None else default_config(**kw)
         rc = _lib.gst_engine_create(device, C.byref(cfg), C.byref(self._h))
         if rc:
@@ -392,6 +394,8 @@ class Engine:
 
     def close(self):
         if self._h:
+            for dg in list(self._graphs):
+                dg.close()
             _lib.gst_engine_destroy(self._h)
             self._h = _vp()
 
@@ -406,16 +410,27 @@ class Engine:
 
 
 class DeviceGraph:
-    """A graph and its groups resident on the engine's device."""
+    """A graph and its groups resident on the engine's device.  With `i64` = (beg_pos,
+    csr, weight) int64 arrays (the reference's _beg_pos/_csr/_weight.bin as read) the
+    graph goes through gst_graph_create_i64 instead, and `g` may be None."""
 
-    def __init__(self, eng: Engine, g: Graph, groups: Groups):
+    def __init__(self, eng: Engine, g: Graph | None, groups: Groups, i64=None):
         self.eng, self.g, self.groups = eng, g, groups
         self._g, self._grp = _vp(), _vp()
-        hg = g.host()
-        rc = _lib.gst_graph_create(eng._h, g.V, g.E, hg.beg_pos, hg.adj, hg.weight,
-                                   C.byref(self._g))
-        if rc:
-            raise GstError(f"gst_graph_create: {STATUS.get(rc, rc)}: {eng.error()}")
+        self._servers = weakref.WeakSet()  # closed before the graph
+        eng._graphs.add(self)
+        if i64 is not None:
+            beg, csr, wt = (np.ascontiguousarray(a, dtype=np.int64) for a in i64)
+            rc = _lib.gst_graph_create_i64(eng._h, beg.shape[0] - 1, csr.shape[0], beg.ctypes.data,
+                                           csr.ctypes.data, wt.ctypes.data, C.byref(self._g))
+            if rc:
+                raise GstError(f"gst_graph_create_i64: {STATUS.get(rc, rc)}: {eng.error()}")
+        else:
+            hg = g.host()
+            rc = _lib.gst_graph_create(eng._h, g.V, g.E, hg.beg_pos, hg.adj, hg.weight,
+                                       C.byref(self._g))
+            if rc:
+                raise GstError(f"gst_graph_create: {STATUS.get(rc, rc)}: {eng.error()}")
         gr = groups.host()
         rc = _lib.gst_groups_create(self._g, gr.n_groups, gr.grp_ptr, gr.members,
                                     C.byref(self._grp))
@@ -447,6 +462,8 @@ class DeviceGraph:
         return n.value
 
     def close(self):
+        for sv in list(self._servers):
+            sv.close()
         if self._grp:
             _lib.gst_groups_destroy(self._grp)
             self._grp = _vp()
@@ -515,6 +532,7 @@ class Server:
     def __init__(self, dg: DeviceGraph):
         self.dg = dg
         self._h = _vp()
+        dg._servers.add(self)
         rc = _lib.gst_server_create(dg._g, dg._grp, C.byref(self._h))
         if rc:
             raise GstError(f"gst_server_create: {STATUS.get(rc, rc)}: {dg.eng.error()}")

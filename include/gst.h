@@ -124,6 +124,7 @@ void gst_config_default(gst_config* cfg);
 gst_status gst_engine_set_profiling(gst_engine* eng, int32_t bits);
 
 gst_status gst_engine_create(int32_t device, const gst_config* cfg, gst_engine** out);
+/* Refuses (GST_BAD_INPUT) while graphs of the engine are alive: destroy them first. */
 gst_status gst_engine_destroy(gst_engine* eng);
 /* Message of the last failure on this engine (thread-local copy; never NULL). */
 const char* gst_last_error_string(gst_engine* eng);
@@ -210,26 +211,36 @@ gst_status gst_wait(gst_server* s, uint64_t ticket, gst_result* res);
 gst_status gst_server_destroy(gst_server* s);
 
 /* Diagnostics (no counterpart in the reference): copy the first n_cells packed
- * state cells (cost<<32 | pending<<31 | parent) of a query slot and the packed
+ * state cells (cost<<32 | pending<<31 | parent) of a query slot's row pool (rows of
+ * 2^k x (D+1) cells in the order the query's vertices took them) and the packed
  * best full-set state (cost<<32 | hop<<27 | vertex) of the query last run in it. */
 gst_status gst_debug_slot_state(gst_graph* g, int32_t slot, uint64_t* cells, int64_t n_cells,
                                 uint64_t* best_out);
 
 /* No-allocation solve (no counterpart in the reference; added for callers that
  * may not allocate device memory).  Some hosts own all device memory through their
- * own pool and forbid a library from calling cudaMalloc/cudaFree, which would also
- * synchronise the device.  This entry point runs one query like gst_solve but
- * allocates nothing: the graph (d_beg_pos[V+1]; d_edges[2E] = neighbour, weight
- * interleaved, sorted by neighbour per vertex, weights >= 1) and the groups
- * (d_grp_ptr[n_groups+1], d_members) are the caller's, already in device memory;
- * the tree is written into the caller's host arrays res->edge_u/edge_v/edge_w of
- * edge_cap entries each (do not call gst_result_free on this result).  All scratch
- * lives in a static device array of GST_NOALLOC_SCRATCH_BYTES that the library
- * holds on every GPU that loads it until the process exits; a query whose state
- * table and worklists do not fit is rejected with GST_OOM_ADMISSION.  The first
- * call on a device looks the array's address up (issue it before any stream
- * capture).  Calls share the array: calls that overlap on one GPU race, so
- * serialise them.  `stream` is a cudaStream_t (NULL = legacy default stream). */
+ * own pool (a database's GPU memory manager, a framework's caching allocator, a
+ * serving process that carves HBM up front) and forbid a library from calling
+ * cudaMalloc/cudaFree, which would also synchronise the device under their other
+ * work.  This entry point runs one query with the same kernels and pruning as
+ * gst_solve but allocates nothing: the graph (d_beg_pos[V+1]; d_edges[2E] =
+ * neighbour, weight interleaved, sorted by neighbour per vertex, weights >= 1) and
+ * the groups (d_grp_ptr[n_groups+1], d_members) are the caller's, already in device
+ * memory; the tree is written into the caller's host arrays res->edge_u/edge_v/edge_w
+ * of edge_cap entries each (do not call gst_result_free on this result; a tree of
+ * more distinct edges than edge_cap returns GST_CAPACITY).  All scratch lives in a
+ * static device array of GST_NOALLOC_SCRATCH_BYTES that the library holds on every
+ * GPU that loads it until the process exits; a query whose state table and worklists
+ * do not fit is rejected with GST_OOM_ADMISSION (about V <= 150k vertices at k = 3,
+ * fewer for larger k and hop bounds).  Without the caller's light-edge index every
+ * relaxation reads a vertex's whole edge list, so large graphs run slower than with
+ * gst_solve.  The first call on a device looks the array's address up and creates two
+ * timing events (issue it before any stream capture).  Calls share the array, which
+ * keeps the previous call's contents (each call clears what must start empty): work
+ * of two calls that overlapped on one GPU would race, so the library serialises its
+ * calls with a process-wide lock and each call returns only after its GPU work is
+ * done.  `stream` is a cudaStream_t (NULL = legacy default stream).  Every failure
+ * is also stored in res->status; the caller's current device is left as it was. */
 #define GST_NOALLOC_SCRATCH_BYTES (64ll << 20)
 gst_status gst_solve_noalloc(int32_t device, void* stream, int64_t V, int64_t E,
                              const int64_t* d_beg_pos, const int32_t* d_edges, int32_t n_groups,

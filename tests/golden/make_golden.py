@@ -8,8 +8,9 @@ oracle/_ref/) on seeded synthetic inputs written in the reference's file formats
 Each fixture records how to regenerate its inputs (generator + seeds), a
 fingerprint of the generated arrays (so generator drift is caught), the queries,
 and the costs the reference printed in its result CSVs (100000 = no solution).
-Only this script and the oracle need /root/reference; the committed JSON is all
-the tests read.
+Only this script and the oracle's build need the reference checkout (its code/
+directory: GST_REFERENCE_CODE, else "reference" beside this repository); the
+committed JSON is all the tests read.
 """
 from __future__ import annotations
 
@@ -85,26 +86,91 @@ SPECS = [
      "solvers": ["PrunedDP++", "D-PrunedDP++"]},
 ]
 
+# The benchmark configurations themselves (bench.py WORKLOADS, same generator calls and
+# seeds): the first queries of each query pool, solved by the reference's multi-core
+# CPU solvers, plus a few by its single-thread PrunedDP++ as a second opinion.
+SEED = 0x6057
+BENCH_SPECS = [
+    # mid-scale plain path: R-MAT 170k target / 6.8M edges, largest component kept
+    {"name": "c2_rmat170k_k5k7",
+     "graph": {"kind": "rmat", "V": 170_000, "E": 6_800_000, "seed": SEED + 2},
+     "groups": {"kind": "zipf", "n": 5000, "s": 1.5, "smin": 2, "smax": 500, "seed": SEED + 1002},
+     "queries": [{"k": 5, "n": 16, "seed": SEED + 2002, "hop": [None]},
+                 {"k": 7, "n": 8, "seed": SEED + 2003, "hop": [None]}],
+     "solvers": ["TrimCDP-multi-core-CPU", "PrunedDP++"],
+     # single-thread PrunedDP++: 80-125 s per k = 5 query here, 700-830 s per k = 7 query
+     "limit": {"PrunedDP++": 2}},
+    # diameter-bounded path: R-MAT grown until the kept component has ~1M vertices and
+    # ~15M edges; k = 5 at D = 3, 4, 5
+    {"name": "c3_rmat1M_k5_D345",
+     "graph": {"kind": "rmat", "V": 2_000_000, "E": 15_300_000, "seed": SEED + 3},
+     "groups": {"kind": "zipf", "n": 10000, "s": 1.5, "smin": 2, "smax": 1000, "seed": SEED + 1003},
+     "queries": [{"k": 5, "n": 4, "seed": SEED + 2031, "hop": [3, 4, 5]}],
+     "solvers": ["D-TrimCDP-multi-core-CPU", "D-PrunedDP++"],
+     "limit": {"D-PrunedDP++": 1}, "per_query": True, "timeout": 1800},
+    # batched configuration: R-MAT grown until the kept component has ~4M vertices and
+    # ~71M edges; k = 3, 5 unbounded and D = 4, k = 7 unbounded
+    {"name": "c4_rmat4M_k357",
+     "graph": {"kind": "rmat", "V": 8_650_000, "E": 71_000_000, "seed": SEED + 4},
+     "groups": {"kind": "zipf", "n": 20000, "s": 1.5, "smin": 2, "smax": 2000, "seed": SEED + 1004},
+     "queries": [{"k": 3, "n": 4, "seed": SEED + 2041, "hop": [None, 4]},
+                 {"k": 5, "n": 4, "seed": SEED + 2042, "hop": [None, 4]},
+                 {"k": 7, "n": 3, "seed": SEED + 2043, "hop": [None]}],
+     "solvers": ["TrimCDP-multi-core-CPU", "D-TrimCDP-multi-core-CPU"],
+     "per_query": True, "timeout": 1800},
+]
+
 
 def run_spec(spec):
+    """Run the spec's solvers on its queries.  A solver listed in spec["limit"] runs
+    on the first `limit` queries of each case only (single-thread solvers at the larger
+    configurations); with spec["per_query"] every query is its own solver run under
+    spec["timeout"] seconds, and a query that runs out of time records no cost (None).
+    Each case also records the solver's own per-query time (its result CSV's time
+    column, main loop only) under "ref_time"."""
     g, grp = make_inputs(spec)
     out = {"name": spec["name"], "graph": spec["graph"], "groups": spec["groups"],
            "V": g.V, "E": g.E, "fingerprint": fingerprint(g, grp), "cases": []}
+    limits = spec.get("limit", {})
+    per_query = spec.get("per_query", False)
+    timeout = spec.get("timeout")
     with tempfile.TemporaryDirectory() as d:
         for qs in spec["queries"]:
             q = G.synth_queries(grp.n_groups, qs["n"], qs["k"], qs["seed"])
             G.write_reference_files(d, "fx", g, grp, q)
             for hop in qs["hop"]:
                 case = {"k": qs["k"], "hop": hop, "query_seed": qs["seed"],
-                        "queries": q.tolist(), "ref": {}}
+                        "queries": q.tolist(), "ref": {}, "ref_time": {}}
                 for s in spec["solvers"]:
                     is_hop = O.REF_SOLVERS[s][1]
                     if is_hop != (hop is not None):
                         continue
-                    rows, wall = O.run_ref(s, d, "fx", qs["k"], 0, qs["n"] - 1, hop_bound=hop)
-                    rows.sort(key=lambda r: r["task_id"])
-                    case["ref"][s] = [r["cost"] for r in rows]
-                    print(spec["name"], "k", qs["k"], "hop", hop, s, f"{wall:.1f}s", flush=True)
+                    n = min(qs["n"], limits.get(s, qs["n"]))
+                    if per_query:
+                        costs, times = [], []
+                        for i in range(n):
+                            try:
+                                rows, wall = O.run_ref(s, d, "fx", qs["k"], i, i, hop_bound=hop,
+                                                       timeout=timeout)
+                                costs.append(rows[0]["cost"])
+                                times.append(rows[0]["time"])
+                            except Exception as e:  # noqa: BLE001 (timeout or failure)
+                                print(spec["name"], s, "query", i, "gave no cost:", type(e).__name__,
+                                      flush=True)
+                                costs.append(None)
+                                times.append(None)
+                                wall = float("nan")
+                            print(spec["name"], "k", qs["k"], "hop", hop, s, "query", i,
+                                  costs[-1], f"{wall:.1f}s", flush=True)
+                    else:
+                        rows, wall = O.run_ref(s, d, "fx", qs["k"], 0, n - 1, hop_bound=hop,
+                                               timeout=timeout)
+                        rows.sort(key=lambda r: r["task_id"])
+                        costs = [r["cost"] for r in rows]
+                        times = [r["time"] for r in rows]
+                        print(spec["name"], "k", qs["k"], "hop", hop, s, f"{wall:.1f}s", flush=True)
+                    case["ref"][s] = costs
+                    case["ref_time"][s] = times
                 out["cases"].append(case)
     return out
 
@@ -137,9 +203,12 @@ KNOWN_ANSWER = {
 
 
 def main(names=None):
-    """Regenerate every fixture, or only the named ones."""
-    fixtures = [run_spec(s) for s in SPECS if not names or s["name"] in names]
-    for f in fixtures:
+    """Regenerate every small fixture, or only the named ones (the benchmark-size
+    fixtures of BENCH_SPECS are made only when named: they take minutes to hours)."""
+    specs = [s for s in SPECS if not names or s["name"] in names]
+    specs += [s for s in BENCH_SPECS if names and s["name"] in names]
+    for spec in specs:
+        f = run_spec(spec)
         with open(os.path.join(HERE, f["name"] + ".json"), "w") as fh:
             json.dump(f, fh, separators=(",", ":"))
     if not names:

@@ -24,18 +24,47 @@ def _check(g, grp, q, hop, a, expect):
         assert rc == 0, (q, hop, G.VERIFY_CODES[rc])
 
 
-@pytest.mark.parametrize("name", ["c1_ba20k_k3", "rmat3k_k4_k5", "rmat20k_k6", "rmat50k_hop",
-                                  "rmat4k_k7_k8"])
+def consensus(case):
+    """Per query of a fixture case, the cost every solver that answered it printed
+    (None when none did); solvers that disagree fail the test."""
+    out = []
+    for i in range(len(case["queries"])):
+        vals = {s: c[i] for s, c in case["ref"].items() if i < len(c) and c[i] is not None}
+        assert len(set(vals.values())) <= 1, (case["k"], case["hop"], i, vals)
+        out.append(next(iter(vals.values())) if vals else None)
+    return out
+
+
+SMALL_FIXTURES = ["c1_ba20k_k3", "rmat3k_k4_k5", "rmat20k_k6", "rmat50k_hop", "rmat4k_k7_k8"]
+# the benchmark configurations themselves (mid-scale plain path, diameter-bounded path,
+# batched configuration), a sample of their queries each
+BENCH_FIXTURES = ["c2_rmat170k_k5k7", "c3_rmat1M_k5_D345"]
+
+
+@pytest.mark.parametrize("name", SMALL_FIXTURES + BENCH_FIXTURES)
 def test_engine_matches_reference_golden(engine, name):
+    """Every query a fixture's reference solvers answered, one at a time and in one
+    batch (each solver's cost is the same, checked by consensus())."""
     fx = load_golden(name)
     g, grp = golden_inputs(fx)
     dg = engine.graph(g, grp)
     try:
+        qs, hops, want = [], [], []
         for case in fx["cases"]:
-            hop = case["hop"]
-            costs = next(iter(case["ref"].values()))
-            for q, c in zip(case["queries"], costs):
-                _check(g, grp, q, hop, dg.solve(q, hop), _ref(c))
+            for q, c in zip(case["queries"], consensus(case)):
+                if c is not None:
+                    qs.append(q)
+                    hops.append(case["hop"])
+                    want.append(_ref(c))
+        assert qs
+        single = name in SMALL_FIXTURES or len(qs) <= 32
+        if single:
+            for q, h, c in zip(qs, hops, want):
+                _check(g, grp, q, h, dg.solve(q, h), c)
+        for i in range(0, len(qs), 32):
+            for q, h, a, c in zip(qs[i:i + 32], hops[i:i + 32],
+                                  dg.solve_batch(qs[i:i + 32], hops[i:i + 32]), want[i:i + 32]):
+                _check(g, grp, q, h, a, c)
     finally:
         dg.close()
 
@@ -196,3 +225,27 @@ def test_hop_budgets_match_oracle(engine):
                 _check(g, grp, q, h, a, c)
         finally:
             dg.close()
+
+
+def test_wide_rows_match_oracle(engine):
+    """Rows of 2^k x (D+1) cells wider than eight warps' shared memory in the rows kernel
+    (k = 8 at D = 7: 2,048 cells; k = 7 at D = 14: 1,920 cells): the kernel runs fewer
+    warps per CTA.  Alone, and mixed into one batch with narrow queries, against the
+    oracle."""
+    rng = np.random.default_rng(907)
+    g = G.synth_rmat(500, 2500, 901)
+    grp = G.synth_groups_zipf(g.V, 60, 1.5, 1, 12, 902)
+    dg = engine.graph(g, grp)
+    qs, hops, want = [], [], []
+    for k, D in ((8, 7), (7, 14), (3, None), (4, 2), (8, 7)):
+        q = rng.choice(grp.n_groups, size=k, replace=False).astype(np.int32)
+        qs.append(q)
+        hops.append(D)
+        want.append(O.gst_nonhop(g, grp, q)["cost"] if D is None else O.gst_hop(g, grp, q, D)["cost"])
+    try:
+        for q, h, c in zip(qs, hops, want):
+            _check(g, grp, q, h, dg.solve(q, h), c)
+        for q, h, a, c in zip(qs, hops, dg.solve_batch(qs, hops), want):
+            _check(g, grp, q, h, a, c)
+    finally:
+        dg.close()

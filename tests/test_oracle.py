@@ -34,6 +34,40 @@ def test_oracle_matches_reference_golden(name):
                 assert o["cost"] == _ref_cost(costs[qi]), (name, solver, case["hop"], qi)
 
 
+ALL_FIXTURES = ["c1_ba20k_k3", "rmat3k_k4_k5", "rmat20k_k6", "rmat50k_hop", "rmat4k_k7_k8",
+                "c2_rmat170k_k5k7", "c3_rmat1M_k5_D345"]
+
+
+@pytest.mark.parametrize("name", ALL_FIXTURES)
+def test_reference_solvers_agree(name):
+    """Where a fixture holds costs from two of the reference's solvers (PrunedDP++ and
+    TrimCDP-multi-core-CPU; D-PrunedDP++ and D-TrimCDP-multi-core-CPU), they agree on
+    every query both answered, and every case has at least one answered query."""
+    fx = load_golden(name)
+    for case in fx["cases"]:
+        answered = 0
+        for i in range(len(case["queries"])):
+            vals = {sv: c[i] for sv, c in case["ref"].items() if i < len(c) and c[i] is not None}
+            assert len(set(vals.values())) <= 1, (name, case["k"], case["hop"], i, vals)
+            answered += bool(vals)
+        assert answered > 0, (name, case["k"], case["hop"])
+
+
+def test_oracle_matches_benchmark_fixture():
+    """The oracle at the mid-scale configuration's size (141k vertices, 13.6M directed
+    edges; the generator's fingerprint checked too): the first k = 5 query."""
+    fx = load_golden("c2_rmat170k_k5k7")
+    g, grp = golden_inputs(fx)
+    per_case = 1
+    for case in fx["cases"][:1]:
+        for i, q in enumerate(case["queries"][:per_case]):
+            vals = [c[i] for c in case["ref"].values() if i < len(c) and c[i] is not None]
+            if not vals:
+                continue
+            o = O.gst_nonhop(g, grp, q) if case["hop"] is None else O.gst_hop(g, grp, q, case["hop"])
+            assert o["cost"] == _ref_cost(vals[0]), (case["hop"], i)
+
+
 def test_oracle_trees_verify():
     fx = load_golden("rmat3k_k4_k5")
     g, grp = golden_inputs(fx)

@@ -30,6 +30,7 @@ _lib.gst_solve_noalloc.argtypes = [C.c_int32, C.c_void_p, C.c_int64, C.c_int64, 
 
 
 def _noalloc(dev, g, grp, q, hop, cap=4096):
+    """One gst_solve_noalloc call; returns (return code, status, cost, edges, root)."""
     eu = np.zeros(cap, np.int32)
     ev = np.zeros(cap, np.int32)
     ew = np.zeros(cap, np.int32)
@@ -90,3 +91,38 @@ def test_noalloc_rejects_oversize():
     rc, st, *_ = _noalloc(dev, g, grp, list(range(8)), None)
     assert rc == G.OOM_ADMISSION and st == G.OOM_ADMISSION
     assert "static scratch" in _lib.gst_last_error_string(None).decode()
+
+
+def test_noalloc_wide_rows_and_statuses(engine):
+    """Hop-bounded rows wider than eight warps' shared memory (k = 8 at D = 7) through the
+    no-allocation solve, the same as gst_solve; a tree with more edges than the caller's
+    arrays hold returns GST_CAPACITY in both the return code and res.status."""
+    import torch
+    import oracle as O
+    rng = np.random.default_rng(911)
+    g = G.synth_rmat(500, 2500, 901)
+    grp = G.synth_groups_zipf(g.V, 60, 1.5, 1, 12, 902)
+    dev = _device_copies(g, grp)
+    torch.cuda.synchronize()
+    dg = engine.graph(g, grp)
+    try:
+        for k, D in ((8, 7), (7, 14), (5, None)):
+            q = rng.choice(grp.n_groups, size=k, replace=False).astype(np.int32)
+            want = O.gst_nonhop(g, grp, q)["cost"] if D is None else O.gst_hop(g, grp, q, D)["cost"]
+            ref = dg.solve(q, D)
+            for call in range(2):
+                rc, st, cost, edges, root = _noalloc(dev, g, grp, q, D)
+                assert st == ref.status and rc == st, (k, D, call, G.STATUS[st])
+                if ref.ok:
+                    assert cost == ref.cost == want, (k, D, cost, ref.cost, want)
+                    vt = G.verify_tree(g, grp, q, -1 if D is None else D, cost, edges, root)
+                    assert vt == 0, G.VERIFY_CODES[vt]
+                else:
+                    assert want == -1
+        q = rng.choice(grp.n_groups, size=6, replace=False).astype(np.int32)
+        ref = dg.solve(q)
+        if ref.ok and len(ref.edges) > 1:
+            rc, st, *_ = _noalloc(dev, g, grp, q, None, cap=1)
+            assert rc == G.CAPACITY and st == G.CAPACITY, (rc, st)
+    finally:
+        dg.close()
