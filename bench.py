@@ -67,6 +67,12 @@ WORKLOADS = {
                groups=("zipf", 20_000, 1.5, 2, 2000, SEED + 1004),
                queries=[(3, 410, SEED + 2041), (5, 410, SEED + 2042), (7, 204, SEED + 2043)],
                hop=(4, 0.5, SEED + 3004), golden="c4_rmat4M_k357"),
+    # the batched form's shape at a quarter of its size (1M-vertex component, 18M
+    # edges): small enough for profiler captures of every kernel
+    "c4q": dict(name="rmat1M_18M_k357_halfD4", graph=("rmat", 2_150_000, 18_000_000, SEED + 4),
+                groups=("zipf", 20_000, 1.5, 2, 2000, SEED + 1004),
+                queries=[(3, 410, SEED + 2041), (5, 410, SEED + 2042), (7, 204, SEED + 2043)],
+                hop=(4, 0.5, SEED + 3004)),
     "c2": dict(name="rmat170k_6.8M_k5k7", graph=("rmat", 170_000, 6_800_000, SEED + 2),
                groups=("zipf", 5000, 1.5, 2, 500, SEED + 1002),
                queries=[(5, 300, SEED + 2002), (7, 300, SEED + 2003)], golden="c2_rmat170k_k5k7"),
@@ -717,6 +723,20 @@ def run_ours(args):
     achieved = kern[top]["GBps"]
     per_launch = kbytes[top] / max(1, klaunch[top])
     traffic, traffic_case = roofline_traffic(top, per_launch)
+    # the ceiling these kernels meet: random 32-byte rows per second (each distance
+    # relaxation reads its target's row, each grow relaxation its target's distance row
+    # and state cell), measured on this device by gst_probe_random_access
+    rand = None
+    try:
+        rand = G.probe_random_access(local_rank, 4 << 30)
+        rand["note"] = ("random 32-byte row gathers from 4 GB (DRAM) and from 32 MB (L2), "
+                        "random 4-byte atomicMin; frac = the kernel's relaxations per second "
+                        "over the DRAM gather rate (one random row per relaxation)")
+        rand["kernels"] = {k: {"relax_per_s": kern[k]["per_s"],
+                               "frac": kern[k]["per_s"] / rand["gather32_dram_per_s"]}
+                           for k in ("k_sssp", "k_grow")}
+    except Exception as e:  # noqa: BLE001 (reported, not fatal)
+        rand = {"error": str(e)}
 
     # parity: the engine's costs against the reference's solvers on the same queries
     parity = {"checked": 0, "agree": 0, "sources": {}}
@@ -771,7 +791,7 @@ def run_ours(args):
                      "note": "algorithmic bytes / event-timed kernel time over a replay of "
                              "the first timed batches; traffic: DRAM bytes per launch from "
                              "the ncu summary in profiles/",
-                     "kernels": kern},
+                     "kernels": kern, "random_access": rand},
         "gpu_launches": launches,
         "clocks": clk.summary(),
     }
@@ -819,6 +839,36 @@ def run_ours(args):
     return 0
 
 
+def run_profile_batch(args):
+    """One batch of the workload's first queries with every level kernel launched on its
+    own (no CUDA graph), after one untimed batch of the same queries; prints the
+    algorithmic bytes and launches per kernel of the second batch as one JSON line.  Run
+    under ncu to relate a kernel's measured DRAM traffic to its algorithmic bytes (the
+    summaries in profiles/ give the commands)."""
+    import gst_b200 as G
+    w, g, grp, queries, hops = make_workload(args.workload)
+    eng = G.Engine(0, max_batch=args.batch, use_graphs=0)
+    dg = eng.graph(g, grp)
+    qs, hs = queries[: args.batch], hops[: args.batch]
+    dg.solve_batch(qs, hs)
+    G.set_profiling(eng, 7)
+    ans = dg.solve_batch(qs, hs)
+    st = ans[0].stats
+    b = level_bytes(ans, qs, hs, 0)
+    out = {"workload": w["name"], "V": g.V, "E_directed": g.E, "batch": len(qs),
+           "kernels": {"k_sssp": {"alg_bytes": b["k_sssp"], "launches": st["sssp_launches"],
+                                  "ms": st["sssp_ms"]},
+                       "k_grow": {"alg_bytes": b["k_grow"], "launches": st["grow_launches"],
+                                  "ms": st["grow_ms"]},
+                       "k_rows": {"alg_bytes": b["k_rows"], "launches": st["rows_launches"],
+                                  "ms": st["rows_ms"]}},
+           "device_ms": st["device_ms"], "costs": [a.cost for a in ans]}
+    print(json.dumps(out))
+    dg.close()
+    eng.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -839,7 +889,12 @@ def main():
     ap.add_argument("--no-graphs", action="store_true",
                     help="host-issued level launches instead of the CUDA-graph loop "
                          "(profilers then see every kernel launch)")
+    ap.add_argument("--profile-batch", action="store_true",
+                    help="one batch of the first --batch queries with per-kernel launches "
+                         "after one untimed batch; prints algorithmic bytes per kernel")
     args = ap.parse_args()
+    if args.profile_batch:
+        return run_profile_batch(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

@@ -22,7 +22,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 CXX = os.environ.get("CXX_HOST", "g++")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU_SOURCES = ["gst_engine.cu"]
+CU_SOURCES = ["gst_engine.cu", "gst_probe.cu"]
 CPP_SOURCES = ["gst_io.cpp", "gst_synth.cpp"]
 HEADERS = ["gst_device.cuh"]
 LIB = os.path.join(HERE, "libgst_b200.so")

@@ -53,7 +53,45 @@ constexpr uint32_t MERGE = 0x40000000u;
 constexpr uint32_t LEAF = 0x3FFFFFFFu;
 constexpr int MAXB = 64;          // queries per batched launch
 constexpr int KMAX = 8;           // groups per query
-constexpr int DIST_STRIDE = 8;    // int32 one-label distances per vertex row
+constexpr int DIST_STRIDE = 8;    // int32 one-label distances per vertex row, at most
+
+// Distance rows are as wide as the query needs: 1, 2, 4 or 8 uint32 (the smallest power
+// of two >= k), so the rows of a query with few groups take less memory and cache (a
+// k = 3 query's rows of a 4M-vertex graph are 64 MB, most of which the L2 holds).
+__host__ __device__ __forceinline__ uint32_t dist_stride(int k) {
+  return k <= 1 ? 1u : k <= 2 ? 2u : k <= 4 ? 4u : 8u;
+}
+// Row v of a distance table of stride ds as eight values (COST_INF past the row).
+__device__ __forceinline__ void load_drow(const uint32_t* base, uint32_t ds, uint64_t v, uint4& a,
+                                          uint4& b) {
+  const uint32_t* p = base + v * ds;
+  b = make_uint4(COST_INF, COST_INF, COST_INF, COST_INF);
+  if (ds == 8u) {
+    a = __ldcg((const uint4*)p);
+    b = __ldcg((const uint4*)p + 1);
+  } else if (ds == 4u) {
+    a = __ldcg((const uint4*)p);
+  } else if (ds == 2u) {
+    const uint2 x = __ldcg((const uint2*)p);
+    a = make_uint4(x.x, x.y, COST_INF, COST_INF);
+  } else {
+    a = make_uint4(__ldcg(p), COST_INF, COST_INF, COST_INF);
+  }
+}
+__device__ __forceinline__ void store_drow(uint32_t* base, uint32_t ds, uint64_t v, const uint4& a,
+                                           const uint4& b) {
+  uint32_t* p = base + v * ds;
+  if (ds == 8u) {
+    ((uint4*)p)[0] = a;
+    ((uint4*)p)[1] = b;
+  } else if (ds == 4u) {
+    *(uint4*)p = a;
+  } else if (ds == 2u) {
+    *(uint2*)p = make_uint2(a.x, a.y);
+  } else {
+    *p = a.x;
+  }
+}
 
 // PH_PREP: distances final; the star bound, group distances and tour table are
 // being built (one k_sssp pass over the distance rows, then the control block).
@@ -117,15 +155,16 @@ struct Ctx {
   uint32_t* rowmap;    // row pool: vertex -> its pool row (ROW_NONE: none yet); nullptr: dense
   uint32_t pool_cap;   // rows of the pool
   uint32_t pool_n;     // pool rows handed out (may exceed pool_cap: ERR_POOL)
-  uint32_t* dist;
+  uint32_t* dist;      // one-label distances: row v at dist + v * ds
+  uint32_t ds;         // uint32 per distance row (dist, snap, dist_h): dist_stride(k)
   uint32_t* rowbits;
   uint32_t* fm[2];     // group-mask frontier (one byte per vertex, four to a word): the
                        // groups whose distance at the vertex improved in the step that
                        // wrote fm[no]; read and cleared by the next step through fm[in_idx]
   uint32_t* snap;      // hop-limited group-mask search: the distance rows of a round's
-                       // frontier as they stood when the round began (V x DIST_STRIDE)
+                       // frontier as they stood when the round began (V rows of ds)
   uint32_t* dist_h;    // hop budgets h = 1..nhb: d_i^{<=h}(v), cheapest paths of at most h
-                       // edges (nhb x V x DIST_STRIDE; budget D is dist itself)
+                       // edges (nhb x V rows of ds; budget D is dist itself)
   uint32_t* tour;      // 2^k x TOUR_STRIDE path table, then 2^k x KMAX row minima
   uint4* q[2];
   uint4* far[2];
@@ -235,10 +274,8 @@ __device__ __forceinline__ uint64_t* row_take(Ctx* c, uint32_t v, uint32_t r) {
 __device__ __forceinline__ void budget_row(const Ctx* c, int64_t V, uint32_t v, int h, uint4& a,
                                            uint4& b) {
   const uint32_t* base = c->dist;
-  if (h >= 1 && h <= c->nhb) base = c->dist_h + (uint64_t)(h - 1) * (uint64_t)V * DIST_STRIDE;
-  const uint4* row = (const uint4*)&base[(uint64_t)v * DIST_STRIDE];
-  a = __ldcg(row);
-  b = __ldcg(row + 1);
+  if (h >= 1 && h <= c->nhb) base = c->dist_h + (uint64_t)(h - 1) * (uint64_t)V * c->ds;
+  load_drow(base, c->ds, v, a, b);
   if (h <= 0) {
     a = make_uint4(a.x ? COST_INF : 0u, a.y ? COST_INF : 0u, a.z ? COST_INF : 0u, a.w ? COST_INF : 0u);
     b = make_uint4(b.x ? COST_INF : 0u, b.y ? COST_INF : 0u, b.z ? COST_INF : 0u, b.w ? COST_INF : 0u);
@@ -558,16 +595,15 @@ struct GroupVecs {
   const uint32_t* v[KMAX];  // d_i(.) of the query's i-th group, V entries each (nullptr:
                             // not cached, left unreached for the distance search)
 };
-// rows: V x DIST_STRIDE distance rows (the distance table, or one hop budget's table)
-__global__ void k_gather_dist(uint32_t* rows, int k, GroupVecs gv, int64_t V) {
+// rows: V distance rows of stride ds (the distance table, or one hop budget's table)
+__global__ void k_gather_dist(uint32_t* rows, uint32_t ds, int k, GroupVecs gv, int64_t V) {
   for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < V;
        v += (int64_t)gridDim.x * blockDim.x) {
     uint32_t d[KMAX];
 #pragma unroll
     for (int i = 0; i < KMAX; i++) d[i] = i < k && gv.v[i] ? __ldg(&gv.v[i][v]) : COST_INF;
-    uint4* row = (uint4*)&rows[(uint64_t)v * DIST_STRIDE];
-    row[0] = make_uint4(d[0], d[1], d[2], d[3]);
-    row[1] = make_uint4(d[4], d[5], d[6], d[7]);
+    store_drow(rows, ds, (uint64_t)v, make_uint4(d[0], d[1], d[2], d[3]),
+               make_uint4(d[4], d[5], d[6], d[7]));
   }
 }
 
@@ -589,9 +625,9 @@ __global__ void k_init(Ctx* ctxs, int nctx, DevGraph G, const int64_t* grp_ptr,
         atomicMin((unsigned long long*)&row[1u << i], (unsigned long long)cell0);
         mark_row(c, v);
         if (c->phase == PH_SSSP) {
-          const uint32_t old = atomicMin(&c->dist[(uint64_t)v * DIST_STRIDE + i], 0u);
+          const uint32_t old = atomicMin(&c->dist[(uint64_t)v * c->ds + i], 0u);
           for (int h = 1; h <= c->nhb; h++)
-            c->dist_h[((uint64_t)(h - 1) * (uint64_t)G.V + v) * DIST_STRIDE + i] = 0u;
+            c->dist_h[((uint64_t)(h - 1) * (uint64_t)G.V + v) * c->ds + i] = 0u;
           const int64_t deg = G.beg[v + 1] - G.beg[v];
           if (old != 0u && deg > 0 && c->sssp_mask) {
             // group-mask items: one head item per vertex (hop count 0), the groups in fm
@@ -683,8 +719,8 @@ __global__ void __launch_bounds__(256, 4) k_sssp(Ctx* ctxs, int nctx, DevGraph G
           // round began (the snapshot its expand step took), so that a round extends
           // paths by exactly one edge
           const uint32_t* src = rounds && chunk ? c->snap : c->dist;
-          const uint4* row = (const uint4*)&src[(uint64_t)v * DIST_STRIDE];
-          const uint4 a = __ldcg(row), b = __ldcg(row + 1);
+          uint4 a, b;
+          load_drow(src, c->ds, v, a, b);
           const uint32_t d[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
           ub = sssp_cutoff(c);
           bend = COST_INF;
@@ -702,9 +738,7 @@ __global__ void __launch_bounds__(256, 4) k_sssp(Ctx* ctxs, int nctx, DevGraph G
           if (rounds && !chunk) {
             // expand step of a round: snapshot the row, queue every chunk of the range
             // for the next step, relax nothing (no distance changes in this step)
-            uint4* srow = (uint4*)&c->snap[(uint64_t)v * DIST_STRIDE];
-            srow[0] = a;
-            srow[1] = b;
+            store_drow(c->snap, c->ds, v, a, b);
             if (mk) {
               const int64_t cnt = count_upto(G, v, b1 - b0, ub - mind);
               P.spawn = (uint32_t)((cnt + split - 1) / split);
@@ -716,7 +750,7 @@ __global__ void __launch_bounds__(256, 4) k_sssp(Ctx* ctxs, int nctx, DevGraph G
         }
       } else if (in_bounds(c, v < G.V && g < (uint32_t)c->k, 2)) {
         const int64_t b0 = G.beg[v], b1 = G.beg[v + 1];
-        const uint32_t cur = __ldcg(&c->dist[(uint64_t)v * DIST_STRIDE + g]);
+        const uint32_t cur = __ldcg(&c->dist[(uint64_t)v * c->ds + g]);
         // ub is read once per item (a per-edge read of one word by every thread of
         // a one-query launch is an L2 hot spot); a stale, larger ub prunes less
         ub = sssp_cutoff(c);
@@ -769,14 +803,14 @@ __global__ void __launch_bounds__(256, 4) k_sssp(Ctx* ctxs, int nctx, DevGraph G
         // lies further than ub is pruned whatever the exact distance (for a group-mask
         // item, cost is its smallest distance)
         ok[x] = ok[x] && in_bounds(ctxs + x_qi[x], u < G.V, 4) && nd <= x_ub[x];
-        const uint32_t* drow = ctxs[x_qi[x]].dist + (uint64_t)u * DIST_STRIDE;
+        const uint32_t xds = ctxs[x_qi[x]].ds;
+        const uint32_t* dbase = ctxs[x_qi[x]].dist;
         ra[x] = make_uint4(0u, 0u, 0u, 0u);
         rb[x] = make_uint4(COST_INF, COST_INF, COST_INF, COST_INF);
         if (ok[x] && (x_gi[x] & SSSP_MASKED)) {
-          ra[x] = __ldcg((const uint4*)drow);
-          if (((x_gi[x] >> 24) & 0xFu) > 4u) rb[x] = __ldcg((const uint4*)drow + 1);
+          load_drow(dbase, xds, u, ra[x], rb[x]);
         } else if (ok[x]) {
-          ra[x].x = __ldcg(drow + (x_gi[x] & 0xFFu));
+          ra[x].x = __ldcg(dbase + (uint64_t)u * xds + (x_gi[x] & 0xFFu));
         }
       }
 #pragma unroll
@@ -799,14 +833,14 @@ __global__ void __launch_bounds__(256, 4) k_sssp(Ctx* ctxs, int nctx, DevGraph G
             if (i < k && od[i] < lim && w <= lim - od[i]) {
               const uint32_t ndi = od[i] + w;
               if (ndi < cu[i]) {
-                const uint32_t old = atomicMin(&c->dist[(uint64_t)u * DIST_STRIDE + i], ndi);
+                const uint32_t old = atomicMin(&c->dist[(uint64_t)u * c->ds + i], ndi);
                 if (ndi < old) {
                   imp |= 1u << i;
                   if (ndi < lim) ext |= 1u << i;
                   // a path of hops + 1 edges (hop-limited rounds): a candidate for every
                   // budget from hops + 1 on
                   for (int h = (int)((x_gi[x] >> SSSP_HOP_SHIFT) & 0xFFu) + 1; h <= c->nhb; h++)
-                    atomicMin(&c->dist_h[((uint64_t)(h - 1) * (uint64_t)G.V + u) * DIST_STRIDE + i],
+                    atomicMin(&c->dist_h[((uint64_t)(h - 1) * (uint64_t)G.V + u) * c->ds + i],
                               ndi);
                 }
                 cu[i] = min(ndi, old);
@@ -840,13 +874,13 @@ __global__ void __launch_bounds__(256, 4) k_sssp(Ctx* ctxs, int nctx, DevGraph G
           }
         } else if (ok[x] && nd < ra[x].x) {
           const uint32_t grp = x_gi[x] & 0xFFu;
-          const uint32_t old = atomicMin(&c->dist[(uint64_t)u * DIST_STRIDE + grp], nd);
+          const uint32_t old = atomicMin(&c->dist[(uint64_t)u * c->ds + grp], nd);
           if (nd < old) {
             // star bound from tentative distances: the k paths found so far from u
             // to a member of each group form a connected subgraph covering every
             // group, so their total length is a feasible cost
-            const uint4* row = (const uint4*)&c->dist[(uint64_t)u * DIST_STRIDE];
-            const uint4 a = __ldcg(row), b = __ldcg(row + 1);
+            uint4 a, b;
+            load_drow(c->dist, c->ds, u, a, b);
             const uint32_t d[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
             const int k = c->k;
             uint64_t sum = 0;
@@ -883,8 +917,8 @@ __global__ void __launch_bounds__(256, 4) k_sssp(Ctx* ctxs, int nctx, DevGraph G
     const int hs = c->hop && c->sssp_hops && c->D / 2 <= c->nhb ? c->D / 2 : -1;
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < G.V;
          v += (int64_t)gridDim.x * blockDim.x) {
-      const uint4* row = (const uint4*)&c->dist[(uint64_t)v * DIST_STRIDE];
-      const uint4 a = __ldcg(row), b = __ldcg(row + 1);
+      uint4 a, b;
+      load_drow(c->dist, c->ds, (uint64_t)v, a, b);
       const uint32_t d[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
       uint64_t sum = 0;
 #pragma unroll
@@ -1013,9 +1047,7 @@ __global__ void __launch_bounds__(256, 3) k_grow(Ctx* ctxs, int nctx, DevGraph G
             // hop budget D - d
             budget_row(c, G.V, u, c->D - (int)d, da[x], db[x]);
           } else {
-            const uint4* row = (const uint4*)&c->dist[(uint64_t)u * DIST_STRIDE];
-            da[x] = __ldcg(row);
-            if (c->k > 4) db[x] = __ldcg(row + 1);
+            load_drow(c->dist, c->ds, u, da[x], db[x]);
           }
         }
       }
@@ -1259,7 +1291,7 @@ __global__ void __launch_bounds__(256, 4) k_rows(Ctx* ctxs, int nctx, DevGraph G
     for (int i = 0; i < KMAX; i++) dv[i] = hb[i] = COST_INF;
     const bool budgets = c->use_lb && hop && c->sssp_hops;
     if (c->use_lb) {
-      const uint32_t mine = lane < k ? __ldcg(&c->dist[(uint64_t)v * DIST_STRIDE + lane]) : COST_INF;
+      const uint32_t mine = lane < k ? __ldcg(&c->dist[(uint64_t)v * c->ds + lane]) : COST_INF;
       const uint32_t cut = c->cut;
       lim = cut == COST_INF ? COST_INF : cut + 1u;
 #pragma unroll

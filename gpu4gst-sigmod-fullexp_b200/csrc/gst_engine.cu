@@ -59,6 +59,7 @@ struct SlotMem {
   uint32_t* snap = nullptr;
   uint32_t* dist_h = nullptr;  // hop budgets 1..nhb of the one-label distances
   int nhb = 0;
+  uint32_t ds = 0;             // uint32 per distance row the buffers were carved for
   uint32_t* tour = nullptr;
   uint4* q[2] = {nullptr, nullptr};
   uint4* far[2] = {nullptr, nullptr};
@@ -91,7 +92,7 @@ uint32_t pool_rows(int64_t V, int boost) {
 // Lay out (or, with base == nullptr, only size) a slot of V vertices: a row pool of
 // `rows` rows of rw cells and the per-vertex buffers.
 size_t carve_slot(SlotMem& m, unsigned char* base, int64_t V, size_t rw, uint32_t rows,
-                  uint32_t cap, uint32_t farcap, int nhb) {
+                  uint32_t cap, uint32_t farcap, int nhb, uint32_t ds) {
   size_t off = 0;
   auto take = [&](size_t n) {
     unsigned char* p = base ? base + off : nullptr;
@@ -102,12 +103,13 @@ size_t carve_slot(SlotMem& m, unsigned char* base, int64_t V, size_t rw, uint32_
   m.table_dirty = m.table_bytes;  // fresh memory: cleared before first use
   m.table = (uint64_t*)take(m.table_bytes);
   m.rowmap = (uint32_t*)take((size_t)V * 4);
-  m.dist = (uint32_t*)take((size_t)V * DIST_STRIDE * 4);
+  m.dist = (uint32_t*)take((size_t)V * ds * 4);
+  m.ds = ds;
   m.rowbits = (uint32_t*)take(((size_t)V + 31) / 32 * 4);
   m.fm[0] = (uint32_t*)take(fm_bytes(V));
   m.fm[1] = (uint32_t*)take(fm_bytes(V));
-  m.snap = (uint32_t*)take((size_t)V * DIST_STRIDE * 4);
-  m.dist_h = (uint32_t*)take((size_t)nhb * (size_t)V * DIST_STRIDE * 4);
+  m.snap = (uint32_t*)take((size_t)V * ds * 4);
+  m.dist_h = (uint32_t*)take((size_t)nhb * (size_t)V * ds * 4);
   m.nhb = nhb;
   m.tour = (uint32_t*)take(kTourWords * 4);
   m.q[0] = (uint4*)take((size_t)cap * 16);
@@ -176,6 +178,11 @@ struct gst_graph {
   uint32_t* d_widx = nullptr;
   int64_t max_deg = 0;       // shape of the graph (autotuner cache key)
   int32_t max_w = 0;
+  // Vertices are renumbered on the device by degree, highest first (ties by id), so that
+  // the rows of the vertices most relaxations land on (the high-degree ones) pack into
+  // few cache lines; groups and results are translated at the boundary.
+  std::vector<int32_t> to_dev;    // caller's vertex id -> device id
+  std::vector<int32_t> to_host;   // device id -> caller's vertex id
   std::unique_ptr<Runner> batch;  // runner of gst_solve / gst_solve_batch (slots kept)
 };
 
@@ -353,6 +360,7 @@ struct Job {
   int boost = 0;                 // worklist capacity boost (capacity retries)
   size_t rw = 0;
   int nhb = 0;                   // hop budgets of the one-label distances
+  uint32_t ds = DIST_STRIDE;     // uint32 per distance row
   uint32_t* cache_dst = nullptr; // a group-cache fill: the distances of group gids[0] to
                                  // every vertex go here (V entries), no DP
   std::atomic<bool> done{false};
@@ -459,7 +467,7 @@ struct Runner {
     const int split = eng->cfg.split_degree;
     const uint32_t cap = list_cap(g->V, g->E, j.rw, split, j.boost);
     return carve_slot(tmp, nullptr, g->V, j.rw, pool_rows(g->V, j.boost), cap,
-                      eng->cfg.bucket_delta > 0 ? cap : 0, j.nhb);
+                      eng->cfg.bucket_delta > 0 ? cap : 0, j.nhb, j.ds);
   }
 
   int rw_max() const {
@@ -588,7 +596,8 @@ struct Runner {
     int s = -1;
     for (int i = 0; i < max_slots; i++)
       if (!owner[i] && mem[i].base && mem[i].table_bytes >= need_table && mem[i].cap >= cap &&
-          mem[i].farcap >= farcap && mem[i].nhb >= j->nhb && (s < 0 || mem[i].bytes < mem[s].bytes))
+          mem[i].farcap >= farcap && mem[i].nhb >= j->nhb && mem[i].ds >= j->ds &&
+          (s < 0 || mem[i].bytes < mem[s].bytes))
         s = i;
     if (s < 0) {
       for (int i = 0; i < max_slots && s < 0; i++)
@@ -603,7 +612,8 @@ struct Runner {
       if (st != GST_OK) return st;
       if (!p) return GST_NOT_READY;
       SlotMem m;
-      carve_slot(m, (unsigned char*)p, g->V, j->rw, pool_rows(g->V, j->boost), cap, farcap, j->nhb);
+      carve_slot(m, (unsigned char*)p, g->V, j->rw, pool_rows(g->V, j->boost), cap, farcap, j->nhb,
+                 j->ds);
       m.base = p;
       m.bytes = need;
       mem[s] = m;
@@ -617,6 +627,7 @@ struct Runner {
     c.table = m.table;
     c.rowmap = m.rowmap;
     c.dist = m.dist;
+    c.ds = j->ds;
     c.rowbits = m.rowbits;
     c.fm[0] = m.fm[0];
     c.fm[1] = m.fm[1];
@@ -680,23 +691,23 @@ struct Runner {
     m.table_dirty = 0;
     if (c.rowmap) CK(cudaMemsetAsync(m.rowmap, 0xFF, (size_t)g->V * 4, st));
     CK(cudaMemsetAsync(m.rowbits, 0, ((size_t)g->V + 31) / 32 * 4, st));
-    if (c.use_lb && !cached) CK(cudaMemsetAsync(m.dist, 0xFF, (size_t)g->V * DIST_STRIDE * 4, st));
+    if (c.use_lb && !cached) CK(cudaMemsetAsync(m.dist, 0xFF, (size_t)g->V * c.ds * 4, st));
     CK(cudaMemsetAsync(m.fm[0], 0, fm_bytes(g->V), st));
     CK(cudaMemsetAsync(m.fm[1], 0, fm_bytes(g->V), st));
     if (c.nhb && !cached)
-      CK(cudaMemsetAsync(m.dist_h, 0xFF, (size_t)c.nhb * (size_t)g->V * DIST_STRIDE * 4, st));
+      CK(cudaMemsetAsync(m.dist_h, 0xFF, (size_t)c.nhb * (size_t)g->V * c.ds * 4, st));
     CK(cudaMemcpyAsync(d_ctx + s, &c, sizeof(Ctx), cudaMemcpyHostToDevice, st));
     cs.h2d += sizeof(Ctx) + sizeof(int32_t) * q->k;
     const DevGraph G = dev_graph(g);
     if (cached) {
-      k_gather_dist<<<eng->sssp_blocks, 256, 0, st>>>(m.dist, q->k, gv, g->V);
+      k_gather_dist<<<eng->sssp_blocks, 256, 0, st>>>(m.dist, c.ds, q->k, gv, g->V);
       cs.launches += 1;
       if (hop)
         for (int h = 1; h <= c.nhb; h++) {
           GroupVecs gh{};
           for (int i = 0; i < q->k; i++) gh.v[i] = hv[i] ? hv[i] + (size_t)(h - 1) * V : nullptr;
           k_gather_dist<<<eng->sssp_blocks, 256, 0, st>>>(
-              m.dist_h + (size_t)(h - 1) * V * DIST_STRIDE, q->k, gh, g->V);
+              m.dist_h + (size_t)(h - 1) * V * c.ds, c.ds, q->k, gh, g->V);
           cs.launches += 1;
         }
     }
@@ -918,12 +929,12 @@ struct Runner {
         if (!c.error && c.phase == PH_DONE) {
           const size_t V = (size_t)g->V;
           CK(cudaMemcpy2DAsync(j->cache_dst + (size_t)c.nhb * V, sizeof(uint32_t), mem[s].dist,
-                               DIST_STRIDE * sizeof(uint32_t), sizeof(uint32_t), V,
+                               (size_t)c.ds * sizeof(uint32_t), sizeof(uint32_t), V,
                                cudaMemcpyDeviceToDevice, eng->stream));
           for (int h = 1; h <= c.nhb; h++)
             CK(cudaMemcpy2DAsync(j->cache_dst + (size_t)(h - 1) * V, sizeof(uint32_t),
-                                 mem[s].dist_h + (size_t)(h - 1) * V * DIST_STRIDE,
-                                 DIST_STRIDE * sizeof(uint32_t), sizeof(uint32_t), V,
+                                 mem[s].dist_h + (size_t)(h - 1) * V * c.ds,
+                                 (size_t)c.ds * sizeof(uint32_t), sizeof(uint32_t), V,
                                  cudaMemcpyDeviceToDevice, eng->stream));
         }
         memset(j->out, 0, sizeof(gst_result));
@@ -954,7 +965,10 @@ struct Runner {
     return write_idle();
   }
 
-  static void fill(const Ctx& c, Job* j, const std::vector<int32_t>& raw, uint32_t nout) {
+  // Result of job j from its context and its raw tree edges (device numbering), in the
+  // caller's vertex ids.
+  void fill(const Ctx& c, Job* j, const std::vector<int32_t>& raw, uint32_t nout) const {
+    const std::vector<int32_t>& host_id = g->to_host;
     gst_result* r = j->out;
     memset(r, 0, sizeof(*r));
     r->user_tag = j->q.user_tag;
@@ -971,13 +985,13 @@ struct Runner {
         std::chrono::duration<double, std::milli>(Clock::now() - j->t_submit).count();
     if (r->status != GST_OK) return;
     r->cost = (int32_t)(c.best >> 32);
-    r->root = (int32_t)(c.best & 0x7FFFFFFull);
+    r->root = host_id[(size_t)(c.best & 0x7FFFFFFull)];
     r->root_hop = (int32_t)((c.best >> 27) & 31u);
     // distinct edges, (min, max) orientation
     std::vector<std::pair<std::pair<int32_t, int32_t>, int32_t>> es;
     es.reserve(nout);
     for (size_t i = 0; i < nout; i++) {
-      int32_t a = raw[3 * i], b = raw[3 * i + 1];
+      int32_t a = host_id[(size_t)raw[3 * i]], b = host_id[(size_t)raw[3 * i + 1]];
       if (a > b) std::swap(a, b);
       es.push_back({{a, b}, raw[3 * i + 2]});
     }
@@ -1022,6 +1036,7 @@ void make_job(Job& j, const gst_query* q, gst_result* r) {
   j.t_submit = Clock::now();
   j.rw = row_width(q->k, q->hop_bound);
   j.nhb = hop_budgets(q->hop_bound);
+  j.ds = dist_stride(q->k);
 }
 
 }  // namespace
@@ -1250,6 +1265,29 @@ static gst_status graph_create_impl(gst_engine* eng, int64_t V, int64_t E, const
   if (beg[0] != 0 || beg[V] != E) return fail(eng, GST_BAD_INPUT, "graph: beg_pos[0] must be 0 and beg_pos[V] == E");
   for (int64_t v = 0; v < V; v++)
     if (beg[v + 1] < beg[v]) return fail(eng, GST_BAD_INPUT, "graph: beg_pos not monotone");
+  for (int64_t i = 0; i < E; i++)
+    if (adj[i] < 0 || adj[i] >= V) return fail(eng, GST_BAD_INPUT, "graph: neighbour id out of range");
+  // device numbering: by degree, highest first, ties by id
+  std::vector<int32_t> to_host((size_t)V), to_dev((size_t)V);
+  for (int64_t v = 0; v < V; v++) to_host[v] = (int32_t)v;
+  std::stable_sort(to_host.begin(), to_host.end(), [&](int32_t a, int32_t b) {
+    return beg[a + 1] - beg[a] > beg[b + 1] - beg[b];
+  });
+  for (int64_t n = 0; n < V; n++) to_dev[to_host[n]] = (int32_t)n;
+  std::vector<int64_t> nbeg((size_t)V + 1, 0);
+  for (int64_t n = 0; n < V; n++) nbeg[n + 1] = nbeg[n] + (beg[to_host[n] + 1] - beg[to_host[n]]);
+  std::vector<int32_t> nadj((size_t)E), nwt((size_t)E);
+#pragma omp parallel for schedule(dynamic, 4096)
+  for (int64_t n = 0; n < V; n++) {
+    const int64_t o = to_host[n];
+    for (int64_t i = beg[o], j = nbeg[n]; i < beg[o + 1]; i++, j++) {
+      nadj[j] = to_dev[adj[i]];
+      nwt[j] = wt[i];
+    }
+  }
+  beg = nbeg.data();
+  adj = nadj.data();
+  wt = nwt.data();
   // Two device copies of the adjacency: sorted by neighbour (edge-weight lookups
   // of the tree walk) and sorted by weight, with per vertex the number of edges of
   // weight <= widx_threshold(t) (t < WIDX), so that a grow step reads only the edges light enough
@@ -1290,6 +1328,8 @@ static gst_status graph_create_impl(gst_engine* eng, int64_t V, int64_t E, const
   g->eng = eng;
   g->V = V;
   g->E = E;
+  g->to_dev.swap(to_dev);
+  g->to_host.swap(to_host);
   for (int64_t v = 0; v < V; v++) g->max_deg = std::max(g->max_deg, beg[v + 1] - beg[v]);
   for (int64_t i = 0; i < E; i++) g->max_w = std::max(g->max_w, wt[i]);
   CK(cudaMalloc(&g->d_beg, sizeof(int64_t) * (V + 1)));
@@ -1368,12 +1408,14 @@ gst_status gst_groups_create(gst_graph* g, int32_t n_groups, const int64_t* grp_
   gr->g = g;
   gr->n = n_groups;
   gr->h_ptr.assign(grp_ptr, grp_ptr + n_groups + 1);
+  std::vector<int32_t> dm((size_t)M);  // members in the graph's device numbering
+  for (int64_t j = 0; j < M; j++) dm[j] = g->to_dev[members[j]];
   CK(cudaMalloc(&gr->d_ptr, sizeof(int64_t) * (n_groups + 1)));
   CK(cudaMalloc(&gr->d_mem, sizeof(int32_t) * std::max<int64_t>(M, 1)));
   CK(cudaMemcpyAsync(gr->d_ptr, grp_ptr, sizeof(int64_t) * (n_groups + 1),
                      cudaMemcpyHostToDevice, eng->stream));
   if (M)
-    CK(cudaMemcpyAsync(gr->d_mem, members, sizeof(int32_t) * M, cudaMemcpyHostToDevice,
+    CK(cudaMemcpyAsync(gr->d_mem, dm.data(), sizeof(int32_t) * M, cudaMemcpyHostToDevice,
                        eng->stream));
   CK(cudaStreamSynchronize(eng->stream));
   *out = gr;
@@ -2087,7 +2129,8 @@ gst_status noalloc_solve(int device, cudaStream_t st, int64_t V, int64_t E, cons
     return o;
   };
   const size_t o_table = take(Vs * RW * 8);
-  const size_t o_dist = take(Vs * DIST_STRIDE * 4);
+  const size_t ds = dist_stride(q->k);
+  const size_t o_dist = take(Vs * ds * 4);
   const size_t o_bits = take((Vs + 31) / 32 * 4);
   const size_t o_rows = take(Vs * 4);
   const size_t o_out = take((size_t)kNoallocOutCap * 12);
@@ -2095,8 +2138,8 @@ gst_status noalloc_solve(int device, cudaStream_t st, int64_t V, int64_t E, cons
   const size_t o_tour = take(kTourWords * 4);
   const size_t o_fm0 = take(fm_bytes(V));
   const size_t o_fm1 = take(fm_bytes(V));
-  const size_t o_snap = take(c.sssp_mask == 2u ? Vs * DIST_STRIDE * 4 : 0);
-  const size_t o_dh = take((size_t)nhb * Vs * DIST_STRIDE * 4);
+  const size_t o_snap = take(c.sssp_mask == 2u ? Vs * ds * 4 : 0);
+  const size_t o_dh = take((size_t)nhb * Vs * ds * 4);
   // four worklists (near and far, ping-pong) of at least 4V + 4096 items each
   const size_t min_lists = 4 * (4 * Vs + 4096) * 16;
   if (off + min_lists > kNoallocScratchBytes) {
@@ -2147,6 +2190,7 @@ gst_status noalloc_solve(int device, cudaStream_t st, int64_t V, int64_t E, cons
   const int split = cfg.split_degree;
   c.table = (uint64_t*)(base + o_table);
   c.dist = (uint32_t*)(base + o_dist);
+  c.ds = (uint32_t)ds;
   c.rowbits = (uint32_t*)(base + o_bits);
   c.tour = (uint32_t*)(base + o_tour);
   c.fm[0] = (uint32_t*)(base + o_fm0);
@@ -2170,11 +2214,11 @@ gst_status noalloc_solve(int device, cudaStream_t st, int64_t V, int64_t E, cons
   // clear what must start empty (the array keeps the previous call's contents), then
   // upload the context
   NCK(cudaMemsetAsync(c.table, 0xFF, Vs * RW * 8, st));
-  NCK(cudaMemsetAsync(c.dist, 0xFF, Vs * DIST_STRIDE * 4, st));
+  NCK(cudaMemsetAsync(c.dist, 0xFF, Vs * ds * 4, st));
   NCK(cudaMemsetAsync(c.rowbits, 0, (Vs + 31) / 32 * 4, st));
   NCK(cudaMemsetAsync(c.fm[0], 0, fm_bytes(V), st));
   NCK(cudaMemsetAsync(c.fm[1], 0, fm_bytes(V), st));
-  if (nhb) NCK(cudaMemsetAsync(c.dist_h, 0xFF, (size_t)nhb * Vs * DIST_STRIDE * 4, st));
+  if (nhb) NCK(cudaMemsetAsync(c.dist_h, 0xFF, (size_t)nhb * Vs * ds * 4, st));
   NCK(cudaMemcpyAsync(d_ctx, &c, sizeof(Ctx), cudaMemcpyHostToDevice, st));
   // the caller's edges are sorted by neighbour only: no light-edge index
   DevGraph G{V, E, d_beg, (const int2*)d_edges, (const int2*)d_edges, nullptr};

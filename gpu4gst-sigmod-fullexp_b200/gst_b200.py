@@ -321,6 +321,8 @@ _sig("gst_submit", C.c_int, [_vp, C.POINTER(Query), C.POINTER(C.c_uint64)])
 _sig("gst_poll", C.c_int, [_vp, C.c_uint64, C.POINTER(Result)])
 _sig("gst_wait", C.c_int, [_vp, C.c_uint64, C.POINTER(Result)])
 _sig("gst_server_destroy", C.c_int, [_vp])
+_sig("gst_probe_random_access", C.c_int, [C.c_int32, C.c_int64, C.POINTER(C.c_double),
+                                          C.POINTER(C.c_double), C.POINTER(C.c_double)])
 
 C_ABI_SYMBOLS = [
     "gst_config_default", "gst_engine_create", "gst_engine_destroy", "gst_last_error_string",
@@ -328,8 +330,20 @@ C_ABI_SYMBOLS = [
     "gst_groups_destroy", "gst_solve", "gst_solve_batch", "gst_result_free",
     "gst_server_create", "gst_submit", "gst_poll", "gst_wait", "gst_server_destroy",
     "gst_debug_slot_state", "gst_solve_noalloc", "gst_engine_set_profiling", "gst_autotune",
-    "gst_groups_cache_warm", "gst_groups_cache_warm_hop",
+    "gst_groups_cache_warm", "gst_groups_cache_warm_hop", "gst_probe_random_access",
 ]
+
+
+def probe_random_access(device: int = 0, nbytes: int = 4 << 30) -> dict:
+    """Random-access ceilings of the device (include/gst.h: gst_probe_random_access):
+    random 32-byte row gathers per second from `nbytes` and from an L2-resident 32 MB,
+    and random 4-byte atomicMin reductions per second."""
+    g, l2, red = C.c_double(), C.c_double(), C.c_double()
+    rc = _lib.gst_probe_random_access(device, nbytes, C.byref(g), C.byref(l2), C.byref(red))
+    if rc:
+        raise GstError(f"gst_probe_random_access: {STATUS.get(rc, rc)}")
+    return {"gather32_dram_per_s": g.value, "gather32_l2_per_s": l2.value,
+            "red32_dram_per_s": red.value, "bytes": nbytes}
 
 
 def set_profiling(eng: "Engine", bits: int) -> None:

@@ -131,7 +131,9 @@ const char* gst_last_error_string(gst_engine* eng);
 
 /* Graph in CSR with both directions stored (beg_pos[V+1], csr[E], weight[E]);
  * weights must be >= 1.  The caller keeps ownership of its arrays; the engine
- * copies them to the device (adjacency sorted per vertex). */
+ * copies them to the device (adjacency sorted per vertex, vertices renumbered by
+ * degree so that high-degree vertices share cache lines; group members and every
+ * result are translated, so callers only ever see their own vertex ids). */
 gst_status gst_graph_create(gst_engine* eng, int64_t V, int64_t E, const int64_t* beg_pos,
                             const int32_t* csr, const int32_t* weight, gst_graph** out);
 gst_status gst_graph_create_i64(gst_engine* eng, int64_t V, int64_t E, const int64_t* beg_pos,
@@ -213,7 +215,8 @@ gst_status gst_server_destroy(gst_server* s);
 /* Diagnostics (no counterpart in the reference): copy the first n_cells packed
  * state cells (cost<<32 | pending<<31 | parent) of a query slot's row pool (rows of
  * 2^k x (D+1) cells in the order the query's vertices took them) and the packed
- * best full-set state (cost<<32 | hop<<27 | vertex) of the query last run in it. */
+ * best full-set state (cost<<32 | hop<<27 | vertex) of the query last run in it; vertices
+ * here are in the engine's device numbering (by degree, highest first, ties by id). */
 gst_status gst_debug_slot_state(gst_graph* g, int32_t slot, uint64_t* cells, int64_t n_cells,
                                 uint64_t* best_out);
 
@@ -246,6 +249,16 @@ gst_status gst_solve_noalloc(int32_t device, void* stream, int64_t V, int64_t E,
                              const int64_t* d_beg_pos, const int32_t* d_edges, int32_t n_groups,
                              const int64_t* d_grp_ptr, const int32_t* d_members,
                              const gst_query* q, int64_t edge_cap, gst_result* res);
+
+/* Memory-system probe (no counterpart in the reference): the random-access rates that
+ * bound the engine's kernels, measured on `device` with an array of `bytes` (>= 256 MB;
+ * allocated and freed by the call).  *gather_dram: uniformly random 32-byte row reads per
+ * second from the whole array; *gather_l2: the same within 32 MB (an L2-resident set);
+ * *red_dram: random 4-byte atomicMin reductions per second over the whole array.  Every
+ * relaxation of the engine reads a random target's distance row or state cell, so these,
+ * not the streaming copy bandwidth, are the ceilings of its level kernels. */
+gst_status gst_probe_random_access(int32_t device, int64_t bytes, double* gather_dram,
+                                   double* gather_l2, double* red_dram);
 
 #ifdef __cplusplus
 }

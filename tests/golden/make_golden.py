@@ -77,6 +77,12 @@ SPECS = [
      "queries": [{"k": 7, "n": 16, "seed": 113, "hop": [None, 3]},
                  {"k": 8, "n": 10, "seed": 114, "hop": [None, 3]}],
      "solvers": ["PrunedDP++", "TrimCDP-multi-core-CPU", "D-PrunedDP++"]},
+    # the widest hop-bounded rows of the serving configuration's mix: k = 8 at D = 4
+    {"name": "rmat4k_k8_D4",
+     "graph": {"kind": "rmat", "V": 4000, "E": 16000, "seed": 121},
+     "groups": {"kind": "zipf", "n": 300, "s": 1.5, "smin": 2, "smax": 120, "seed": 122},
+     "queries": [{"k": 8, "n": 12, "seed": 123, "hop": [4]}],
+     "solvers": ["D-PrunedDP++", "D-TrimCDP-multi-core-CPU"]},
     # hop-bounded queries at a larger scale (the hop-limited lower bounds prune hard)
     {"name": "rmat50k_hop",
      "graph": {"kind": "rmat", "V": 50000, "E": 400000, "seed": 101},

@@ -35,7 +35,8 @@ def consensus(case):
     return out
 
 
-SMALL_FIXTURES = ["c1_ba20k_k3", "rmat3k_k4_k5", "rmat20k_k6", "rmat50k_hop", "rmat4k_k7_k8"]
+SMALL_FIXTURES = ["c1_ba20k_k3", "rmat3k_k4_k5", "rmat20k_k6", "rmat50k_hop", "rmat4k_k7_k8",
+                  "rmat4k_k8_D4"]
 # the benchmark configurations themselves (mid-scale plain path, diameter-bounded path,
 # batched configuration), a sample of their queries each
 BENCH_FIXTURES = ["c2_rmat170k_k5k7", "c3_rmat1M_k5_D345"]

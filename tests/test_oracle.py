@@ -17,12 +17,12 @@ def _ref_cost(c):
 
 
 @pytest.mark.parametrize("name", ["c1_ba20k_k3", "rmat3k_k4_k5", "rmat20k_k6", "rmat50k_hop",
-                                  "rmat4k_k7_k8"])
+                                  "rmat4k_k7_k8", "rmat4k_k8_D4"])
 def test_oracle_matches_reference_golden(name):
     fx = load_golden(name)
     g, grp = golden_inputs(fx)
     # the larger DPs take about a second per query here
-    limit = {"rmat20k_k6": 10, "rmat50k_hop": 4}.get(name)
+    limit = {"rmat20k_k6": 10, "rmat50k_hop": 4, "rmat4k_k8_D4": 3}.get(name)
     for case in fx["cases"]:
         qs = case["queries"][:limit]
         for solver, costs in case["ref"].items():
@@ -34,7 +34,7 @@ def test_oracle_matches_reference_golden(name):
                 assert o["cost"] == _ref_cost(costs[qi]), (name, solver, case["hop"], qi)
 
 
-ALL_FIXTURES = ["c1_ba20k_k3", "rmat3k_k4_k5", "rmat20k_k6", "rmat50k_hop", "rmat4k_k7_k8",
+ALL_FIXTURES = ["c1_ba20k_k3", "rmat3k_k4_k5", "rmat20k_k6", "rmat50k_hop", "rmat4k_k7_k8", "rmat4k_k8_D4",
                 "c2_rmat170k_k5k7", "c3_rmat1M_k5_D345"]
 
 
