@@ -577,7 +577,7 @@ def run_ours(args):
         tq, th = batch(0)
         tuned = dg.autotune(tq, th, cache_path=cache)
         tuned = {k: tuned[k] for k in ("split_degree", "bucket_delta", "threads_per_block",
-                                       "blocks_per_sm", "max_batch")}
+                                       "blocks_per_sm", "max_batch", "search_cut_permille")}
     for s in range(args.warmup):
         usable(dg.solve_batch(*batch(s)))
 

@@ -193,8 +193,10 @@ struct Ctx {
   uint32_t ub;          // best feasible cost known (one-label solutions and full cells)
   uint32_t cut;         // cutoff when the one-label distances became final: a distance
                         // above it (or unreached) is only known to exceed it
-  uint32_t cut_mult;    // the distance search stops at cut_mult x ub (hop-bounded queries
-                        // prune against their own, larger, bound and want more of them)
+  uint32_t cut_pm;      // the distance search stops at cut_pm / 1000 x ub: below 1000 it
+                        // searches less and leaves weaker (still valid) bounds to the DP;
+                        // hop-bounded queries, which prune against their own larger bound,
+                        // may want more than 1000
   uint32_t sssp_hops;   // 0: distances d_i(v); D: hop-limited distances d_i^{<=D}(v), the
                         // cheapest paths of at most D edges (hop-bounded queries)
   int32_t nhb;          // hop budgets kept in dist_h
@@ -349,17 +351,21 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x) {
 // list under the key cost + weight(next edge), so heavy edges are read only once
 // the frontier has reached their target cost, by which time ub has usually pruned
 // them.  The near list holds items of the current bucket.
-// Distance cutoff of the one-label search: cut_mult x ub, saturating; for hop-limited
-// distances at least the best star of D/2-edge paths, a feasible cost of the query, so
-// that every distance a pruning test can use (up to the query's own bound) is exact.
-// Both terms only decrease, so the cutoff never grows during the search.
+// Distance cutoff of the one-label search: cut_pm / 1000 x ub, saturating; for
+// hop-limited distances ub is at least the best star of D/2-edge paths, a feasible cost
+// of the query.  Both only decrease, so the cutoff never grows during the search.  Any
+// cutoff is valid: a stored distance <= the final cutoff is exact (every prefix of its
+// shortest path stayed below the cutoff) and any other is only known to exceed it, so
+// every bound uses min(d, cut + 1).  A lower cutoff trades search work for DP work.
 __device__ __forceinline__ uint32_t sssp_cutoff(const Ctx* c) {
   if (c->sssp_full) return COST_INF;
-  uint64_t x = (uint64_t)__ldcg(&c->ub) * (c->cut_mult ? c->cut_mult : 1u);
+  uint32_t ub = __ldcg(&c->ub);
   if (c->sssp_hops) {
     const uint32_t h = __ldcg(&c->ub_hop);
-    x = x > h ? x : h;
+    ub = ub > h ? ub : h;
   }
+  if (ub == COST_INF) return COST_INF;
+  const uint64_t x = (uint64_t)ub * (c->cut_pm ? c->cut_pm : 1000u) / 1000u;
   return x >= COST_INF ? COST_INF : (uint32_t)x;
 }
 

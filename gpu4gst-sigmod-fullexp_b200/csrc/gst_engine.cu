@@ -324,7 +324,10 @@ void init_query_ctx(Ctx& c, const gst_query* q, const gst_config& cfg) {
   // hop-bounded queries prune with them against their own bound ub_cell.
   c.use_lb = 1;
   c.use_tour = 1;
-  c.cut_mult = hop ? (uint32_t)(cfg.hop_cut_mult > 0 ? cfg.hop_cut_mult : 1) : 1u;
+  c.cut_pm = hop ? (cfg.hop_cut_permille > 0
+                       ? (uint32_t)cfg.hop_cut_permille
+                       : 1000u * (uint32_t)(cfg.hop_cut_mult > 0 ? cfg.hop_cut_mult : 1))
+                 : (uint32_t)(cfg.search_cut_permille > 0 ? cfg.search_cut_permille : 1000);
   // A tree of diameter <= D reaches every missing group within D edges of any of its
   // vertices, so hop-bounded queries bound with the cheapest paths of at most D
   // edges (a level-synchronous search of D rounds), tighter than unlimited ones.
@@ -1166,6 +1169,7 @@ void gst_config_default(gst_config* cfg) {
   cfg->use_graphs = 1;
   cfg->verbose = 0;
   cfg->hop_cut_mult = 1;
+  cfg->search_cut_permille = 1000;
 }
 
 gst_status gst_engine_create(int32_t device, const gst_config* cfg, gst_engine** out) {
@@ -1189,6 +1193,7 @@ gst_status gst_engine_create(int32_t device, const gst_config* cfg, gst_engine**
     if (eng->cfg.max_batch <= 0) eng->cfg.max_batch = d.max_batch;
     if (eng->cfg.use_graphs < 0) eng->cfg.use_graphs = 0;
     if (eng->cfg.hop_cut_mult <= 0) eng->cfg.hop_cut_mult = 1;
+    if (eng->cfg.search_cut_permille <= 0) eng->cfg.search_cut_permille = 1000;
   }
   // the rows kernel is compiled for at most 256 threads per CTA (4 CTAs per SM)
   eng->cfg.threads_per_block = std::max(64, std::min(256, eng->cfg.threads_per_block / 32 * 32));
@@ -1755,7 +1760,7 @@ std::string shape_key(const gst_graph* g, int32_t max_batch) {
 }
 
 struct TuneParams {
-  int32_t split_degree, bucket_delta, threads_per_block, blocks_per_sm, max_batch;
+  int32_t split_degree, bucket_delta, threads_per_block, blocks_per_sm, max_batch, search_cut;
 };
 
 void set_params(gst_graph* g, const TuneParams& p) {
@@ -1765,6 +1770,7 @@ void set_params(gst_graph* g, const TuneParams& p) {
   eng->cfg.threads_per_block = std::max(64, std::min(256, p.threads_per_block / 32 * 32));
   eng->cfg.blocks_per_sm = p.blocks_per_sm;
   eng->cfg.max_batch = std::max(1, std::min(MAXB, p.max_batch));
+  eng->cfg.search_cut_permille = std::max(1, p.search_cut);
   apply_launch_config(eng);
   g->batch.reset();  // its CUDA graphs hold the old launch geometry
 }
@@ -1781,8 +1787,8 @@ bool read_cache(const char* path, const std::string& key, TuneParams* p) {
     *bar = 0;
     if (key != line) continue;
     TuneParams t;
-    if (sscanf(bar + 1, "%d %d %d %d %d", &t.split_degree, &t.bucket_delta, &t.threads_per_block,
-               &t.blocks_per_sm, &t.max_batch) == 5) {
+    if (sscanf(bar + 1, "%d %d %d %d %d %d", &t.split_degree, &t.bucket_delta, &t.threads_per_block,
+               &t.blocks_per_sm, &t.max_batch, &t.search_cut) == 6) {
       *p = t;
       hit = true;  // the last line for a key wins
     }
@@ -1801,7 +1807,7 @@ extern "C" gst_status gst_autotune(gst_graph* g, gst_groups* grp, int32_t n,
     return fail(eng, GST_BAD_INPUT, "autotune: bad arguments");
   const std::string key = shape_key(g, eng->cfg.max_batch);
   TuneParams cur{eng->cfg.split_degree, eng->cfg.bucket_delta, eng->cfg.threads_per_block,
-                 eng->cfg.blocks_per_sm, eng->cfg.max_batch};
+                 eng->cfg.blocks_per_sm, eng->cfg.max_batch, eng->cfg.search_cut_permille};
   TuneParams hit;
   if (read_cache(cache_path, key, &hit)) {
     std::lock_guard<std::mutex> lk(eng->mu);
@@ -1851,18 +1857,21 @@ extern "C" gst_status gst_autotune(gst_graph* g, gst_groups* grp, int32_t n,
   std::vector<int32_t> c_batch;  // resident queries: at most the configured batch
   for (int32_t b : {1, 2, 4, 8, 16, 32, 64})
     if (b < cur.max_batch) c_batch.push_back(b);
-  for (int param = 0; param < 5 && st == GST_OK; param++) {
-    const std::vector<int32_t>& cand = param == 0   ? c_split
-                                       : param == 1 ? c_delta
-                                       : param == 2 ? c_tpb
-                                       : param == 3 ? c_bps
+  const std::vector<int32_t> c_cut = {1000, 875, 750};  // search cutoff, permille of ub
+  for (int param = 0; param < 6 && st == GST_OK; param++) {
+    const std::vector<int32_t>& cand = param == 0   ? c_cut
+                                       : param == 1 ? c_split
+                                       : param == 2 ? c_delta
+                                       : param == 3 ? c_tpb
+                                       : param == 4 ? c_bps
                                                     : c_batch;
     for (int32_t v : cand) {
       TuneParams p = cur;
-      int32_t* field = param == 0   ? &p.split_degree
-                       : param == 1 ? &p.bucket_delta
-                       : param == 2 ? &p.threads_per_block
-                       : param == 3 ? &p.blocks_per_sm
+      int32_t* field = param == 0   ? &p.search_cut
+                       : param == 1 ? &p.split_degree
+                       : param == 2 ? &p.bucket_delta
+                       : param == 3 ? &p.threads_per_block
+                       : param == 4 ? &p.blocks_per_sm
                                     : &p.max_batch;
       if (*field == v) continue;
       *field = v;
@@ -1884,8 +1893,8 @@ extern "C" gst_status gst_autotune(gst_graph* g, gst_groups* grp, int32_t n,
   if (cache_path) {
     FILE* f = fopen(cache_path, "a");
     if (f) {
-      fprintf(f, "%s|%d %d %d %d %d\n", key.c_str(), cur.split_degree, cur.bucket_delta,
-              cur.threads_per_block, cur.blocks_per_sm, cur.max_batch);
+      fprintf(f, "%s|%d %d %d %d %d %d\n", key.c_str(), cur.split_degree, cur.bucket_delta,
+              cur.threads_per_block, cur.blocks_per_sm, cur.max_batch, cur.search_cut);
       fclose(f);
     }
   }

@@ -273,7 +273,8 @@ class Config(C.Structure):
                 ("threads_per_block", C.c_int32), ("blocks_per_sm", C.c_int32),
                 ("max_batch", C.c_int32), ("use_graphs", C.c_int32),
                 ("profile_kernels", C.c_int32), ("verbose", C.c_int32),
-                ("hop_cut_mult", C.c_int32)]
+                ("hop_cut_mult", C.c_int32), ("search_cut_permille", C.c_int32),
+                ("hop_cut_permille", C.c_int32)]
 
 
 class Query(C.Structure):

@@ -74,6 +74,12 @@ typedef struct gst_config {
   int32_t hop_cut_mult;       /* hop-bounded queries: the distance search stops at this
                                  multiple of the star bound (0 = 1); larger prunes more
                                  DP states and costs a longer search */
+  int32_t search_cut_permille; /* unbounded queries: the distance search stops at this
+                                 many thousandths of the star bound (0 = 1000); less
+                                 searches fewer vertices and leaves weaker, still exact
+                                 bounds to the DP (the autotuner chooses it) */
+  int32_t hop_cut_permille;   /* hop-bounded queries: the same in thousandths (0: use
+                                 hop_cut_mult x 1000) */
 } gst_config;
 
 typedef struct gst_query {

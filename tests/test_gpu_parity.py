@@ -39,7 +39,7 @@ SMALL_FIXTURES = ["c1_ba20k_k3", "rmat3k_k4_k5", "rmat20k_k6", "rmat50k_hop", "r
                   "rmat4k_k8_D4"]
 # the benchmark configurations themselves (mid-scale plain path, diameter-bounded path,
 # batched configuration), a sample of their queries each
-BENCH_FIXTURES = ["c2_rmat170k_k5k7", "c3_rmat1M_k5_D345"]
+BENCH_FIXTURES = ["c2_rmat170k_k5k7", "c3_rmat1M_k5_D345", "c4_rmat4M_k357"]
 
 
 @pytest.mark.parametrize("name", SMALL_FIXTURES + BENCH_FIXTURES)
@@ -250,3 +250,30 @@ def test_wide_rows_match_oracle(engine):
             _check(g, grp, q, h, a, c)
     finally:
         dg.close()
+
+
+@pytest.mark.parametrize("permille", [250, 500])
+def test_search_cutoff_keeps_optima(permille):
+    """A distance search stopped below the star bound (search_cut_permille < 1000) leaves
+    distances above its cutoff clamped to cutoff + 1, weaker but still valid bounds: the
+    optima stay the reference's, alone and in a batch."""
+    eng = G.Engine(0, search_cut_permille=permille, hop_cut_permille=permille, max_batch=16)
+    try:
+        for name in ("rmat3k_k4_k5", "rmat4k_k7_k8", "c1_ba20k_k3", "rmat50k_hop", "rmat4k_k8_D4"):
+            fx = load_golden(name)
+            g, grp = golden_inputs(fx)
+            dg = eng.graph(g, grp)
+            qs, hops, want = [], [], []
+            for case in fx["cases"]:
+                for q, c in list(zip(case["queries"], consensus(case)))[:12]:
+                    if c is not None:
+                        qs.append(q)
+                        hops.append(case["hop"])
+                        want.append(_ref(c))
+            for q, h, a, c in zip(qs, hops, dg.solve_batch(qs, hops), want):
+                _check(g, grp, q, h, a, c)
+            for q, h, c in list(zip(qs, hops, want))[::5]:
+                _check(g, grp, q, h, dg.solve(q, h), c)
+            dg.close()
+    finally:
+        eng.close()

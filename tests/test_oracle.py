@@ -35,7 +35,7 @@ def test_oracle_matches_reference_golden(name):
 
 
 ALL_FIXTURES = ["c1_ba20k_k3", "rmat3k_k4_k5", "rmat20k_k6", "rmat50k_hop", "rmat4k_k7_k8", "rmat4k_k8_D4",
-                "c2_rmat170k_k5k7", "c3_rmat1M_k5_D345"]
+                "c2_rmat170k_k5k7", "c3_rmat1M_k5_D345", "c4_rmat4M_k357"]
 
 
 @pytest.mark.parametrize("name", ALL_FIXTURES)
