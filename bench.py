@@ -577,7 +577,8 @@ def run_ours(args):
         tq, th = batch(0)
         tuned = dg.autotune(tq, th, cache_path=cache)
         tuned = {k: tuned[k] for k in ("split_degree", "bucket_delta", "threads_per_block",
-                                       "blocks_per_sm", "max_batch", "search_cut_permille")}
+                                       "blocks_per_sm", "max_batch", "search_cut_permille",
+                                       "batch_search")}
     for s in range(args.warmup):
         usable(dg.solve_batch(*batch(s)))
 
@@ -692,13 +693,15 @@ def run_ours(args):
     # CUDA-graph loop, which has no per-kernel events)
     peak, peak_kind = peak_hbm()
     G.set_profiling(eng, 7)
-    kms = {"k_grow": 0.0, "k_rows": 0.0, "k_sssp": 0.0}
-    kbytes = {"k_grow": 0.0, "k_rows": 0.0, "k_sssp": 0.0}
-    klaunch = {"k_grow": 0, "k_rows": 0, "k_sssp": 0}
-    # work units per kernel: grow edge relaxations, merged rows, distance relaxations
-    kunits = {"k_grow": 0, "k_rows": 0, "k_sssp": 0}
+    kms = {"k_grow": 0.0, "k_rows": 0.0, "k_sssp": 0.0, "k_bs_relax": 0.0}
+    kbytes = {"k_grow": 0.0, "k_rows": 0.0, "k_sssp": 0.0, "k_bs_relax": 0.0}
+    klaunch = {"k_grow": 0, "k_rows": 0, "k_sssp": 0, "k_bs_relax": 0}
+    # work units per kernel: grow edge relaxations, merged rows, distance relaxations,
+    # target-row sectors of the batch-shared search (its time: the whole shared search,
+    # scans and control included; 32 B per sector read)
+    kunits = {"k_grow": 0, "k_rows": 0, "k_sssp": 0, "k_bs_relax": 0}
     unit_of = {"k_grow": "edge_relaxations", "k_rows": "rows_merged",
-               "k_sssp": "sssp_relaxations"}
+               "k_sssp": "sssp_relaxations", "k_bs_relax": "shared_sectors"}
     for s in range(min(args.steps, 3)):
         qs, hs = batch(args.warmup + s)
         ans = dg.solve_batch(qs, hs)
@@ -706,13 +709,18 @@ def run_ours(args):
         kms["k_grow"] += st["grow_ms"]
         kms["k_rows"] += st["rows_ms"]
         kms["k_sssp"] += st["sssp_ms"]
+        kms["k_bs_relax"] += st["shared_ms"]
         for kname, v in level_bytes(ans, qs, hs, tuned["bucket_delta"] if tuned else 0).items():
             kbytes[kname] += v
+        kbytes["k_bs_relax"] += 32.0 * st["shared_sectors"]
         for kname, field in (("k_grow", "grow_launches"), ("k_rows", "rows_launches"),
-                             ("k_sssp", "sssp_launches")):
+                             ("k_sssp", "sssp_launches"), ("k_bs_relax", "shared_launches")):
             klaunch[kname] += st[field]
         for kname, field in unit_of.items():
-            kunits[kname] += sum(a.stats[field] for a in ans)
+            if kname == "k_bs_relax":
+                kunits[kname] += st[field]
+            else:
+                kunits[kname] += sum(a.stats[field] for a in ans)
     G.set_profiling(eng, 0)
     top = max(kms, key=lambda k: kms[k])
     kern = {k: {"ms": kms[k], "alg_bytes": kbytes[k], "launches": klaunch[k],
@@ -734,7 +742,7 @@ def run_ours(args):
                         "over the DRAM gather rate (one random row per relaxation)")
         rand["kernels"] = {k: {"relax_per_s": kern[k]["per_s"],
                                "frac": kern[k]["per_s"] / rand["gather32_dram_per_s"]}
-                           for k in ("k_sssp", "k_grow")}
+                           for k in ("k_sssp", "k_grow", "k_bs_relax") if kern[k]["ms"] > 0}
     except Exception as e:  # noqa: BLE001 (reported, not fatal)
         rand = {"error": str(e)}
 

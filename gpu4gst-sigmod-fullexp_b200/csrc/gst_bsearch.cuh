@@ -1,0 +1,282 @@
+// Batch-shared one-label distance search.
+//
+// The unbounded queries of one batch call need the distances from each of their groups
+// to every vertex (below a cutoff).  Searching query by query reads the graph's edges and
+// one random 32-byte distance row per relaxation, once per query; the relaxation rate is
+// then bound by the device's random-access rate.  Here the distinct groups of all the
+// batch's unbounded queries (up to BS_COLS of them) are searched together: one distance
+// table of V rows x Gp columns (column c = the c-th group), one announcement bit per
+// (vertex, column), and a relaxation of edge (v, u) serves every column whose distance
+// at v improved in the previous step, reading u's row as one contiguous span (lanes of a
+// warp take its 32-byte sectors) instead of one random row per query.
+//
+// Cutoffs: a query's distances are needed exactly only up to its search cutoff (its star
+// bound x cut_pm / 1000).  Column c keeps the largest cutoff of the queries that use it;
+// stars are found while the search runs (the relax kernel, for each announced vertex,
+// sums each query's columns there) and the cutoffs only decrease, so every distance at
+// most a column's final cutoff is exact (every prefix of its shortest path stayed below
+// it) and every other one is only known to exceed it.  A query then takes the smallest
+// final cutoff of its columns as its own `cut` (distances above it are clamped to cut + 1
+// by every bound), at least as strong as its own search would have reached.
+//
+// Per step: k_bs_scan turns the announcement bits of the previous step into relax items
+// of at most BS_CHUNK edges (a hub's range spread over many warps), k_bs_relax relaxes
+// them, k_bs_ctrl updates the cutoffs and ends the search when nothing was announced.
+#pragma once
+#include "gst_device.cuh"
+
+namespace gst {
+
+constexpr int BS_COLS = 256;   // columns (distinct groups) of one shared search, at most
+constexpr int BS_CHUNK = 64;   // edges per relax item
+constexpr int BS_MAXQ = MAXB;  // queries of one shared search, at most
+
+struct BsCtx {
+  uint32_t* dist;       // V x Gp distances, row v at dist + v * Gp
+  uint32_t* fm[2];      // V x Wm announcement words (bit c: column c improved at v)
+  uint32_t* am;         // V x Wm: v's active columns in the current step (scan -> relax)
+  uint2* items;         // relax items of the current step: {v, chunk}
+  uint32_t item_cap;
+  uint32_t n_items;     // items of the current step (appended by the scan)
+  uint32_t Gp, Wm;      // columns (a multiple of 8), mask words per vertex
+  uint32_t in;          // fm[in] is scanned this step; fm[in ^ 1] takes its announcements
+  uint32_t ann;         // the relax step announced something
+  uint32_t done, steps, max_steps, error;
+  uint32_t cut_pm;      // query cutoff: star x cut_pm / 1000
+  uint32_t nq;          // queries
+  uint32_t qk[BS_MAXQ];
+  uint16_t qcol[BS_MAXQ][KMAX];  // columns of each query's groups
+  uint32_t star[BS_MAXQ];        // best star found per query (a feasible cost)
+  uint32_t cutc[BS_COLS];        // per column: its distance cutoff
+  unsigned long long st_relax;   // target-row sectors read (edges x active lanes)
+};
+constexpr uint32_t BS_ERR_ITEMS = 1, BS_ERR_STEPS = 2;
+
+// Seeds: column c's members at distance 0, announced (blockIdx.y = column).
+__global__ void k_bs_seed(BsCtx* b, DevGraph G, const int64_t* grp_ptr, const int32_t* members,
+                          const int32_t* col_gid, int ncols) {
+  const int c = blockIdx.y;
+  if (c >= ncols) return;
+  const int32_t g = col_gid[c];
+  const uint32_t Gp = b->Gp, Wm = b->Wm;
+  for (int64_t j = grp_ptr[g] + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < grp_ptr[g + 1];
+       j += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t v = (uint32_t)members[j];
+    if (v >= G.V) continue;
+    atomicMin(&b->dist[(uint64_t)v * Gp + c], 0u);
+    if (G.beg[v + 1] > G.beg[v]) atomicOr(&b->fm[b->in][(uint64_t)v * Wm + (c >> 5)], 1u << (c & 31));
+  }
+}
+
+// Scan: every vertex announced in the previous step gets its active columns (moved from
+// fm[in] to am) and one relax item per BS_CHUNK edges of its list.
+__global__ void k_bs_scan(BsCtx* b, DevGraph G) {
+  if (b->done) return;
+  const uint32_t Wm = b->Wm;
+  uint32_t* fi = b->fm[b->in];
+  const int lane = threadIdx.x & 31;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < G.V;
+       base += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t v = base + threadIdx.x;
+    uint32_t nchunks = 0;
+    if (v < G.V) {
+      uint32_t x[BS_COLS / 32];
+      uint32_t any = 0;
+#pragma unroll
+      for (uint32_t w = 0; w < BS_COLS / 32; w++) {
+        x[w] = w < Wm ? __ldcg(&fi[(uint64_t)v * Wm + w]) : 0u;
+        any |= x[w];
+      }
+      if (any) {
+        // the announcements become this step's active columns; the words are cleared
+        // for the step after next
+#pragma unroll
+        for (uint32_t w = 0; w < BS_COLS / 32; w++)
+          if (w < Wm) {
+            b->am[(uint64_t)v * Wm + w] = x[w];
+            fi[(uint64_t)v * Wm + w] = 0u;
+          }
+        const int64_t deg = G.beg[v + 1] - G.beg[v];
+        nchunks = (uint32_t)((deg + BS_CHUNK - 1) / BS_CHUNK);
+      }
+    }
+    // warp-aggregated reservation of the items
+    const uint32_t scan = warp_incl_scan(nchunks);
+    const uint32_t tot = __shfl_sync(0xffffffffu, scan, 31);
+    uint32_t basei = 0;
+    if (lane == 31 && tot) basei = atomicAdd(&b->n_items, tot);
+    basei = __shfl_sync(0xffffffffu, basei, 31);
+    for (uint32_t j = 0; j < nchunks; j++) {
+      const uint32_t i = basei + scan - nchunks + j;
+      if (i < b->item_cap) b->items[i] = make_uint2((uint32_t)v, j);
+      else atomicOr(&b->error, BS_ERR_ITEMS);
+    }
+  }
+}
+
+// Relax: one item per warp iteration.  Lane s holds columns 8s..8s+7 of the item's
+// vertex (its distances, cutoffs and active bits); for each edge of the item's chunk the
+// lanes with active columns read their sector of the target's row, relax, and announce
+// the improved columns.  The first chunk of a vertex also sums each query's columns
+// there (a star: the query's k shortest paths from v form a connected subgraph covering
+// every group, a feasible cost).
+__global__ void __launch_bounds__(256, 4) k_bs_relax(BsCtx* b, DevGraph G) {
+  __shared__ uint32_t s_cut[BS_COLS];
+  __shared__ uint32_t s_row[256 / 32][BS_COLS];  // per warp: the first chunk's full row
+  if (b->done) return;
+  const uint32_t Gp = b->Gp, Wm = b->Wm, nsec = Gp / 8u, nq = b->nq;
+  for (uint32_t c = threadIdx.x; c < BS_COLS; c += blockDim.x) s_cut[c] = c < Gp ? b->cutc[c] : 0u;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const uint32_t n = min(b->n_items, b->item_cap);
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  uint32_t* dist = b->dist;
+  uint32_t* fo = b->fm[b->in ^ 1u];
+  // per lane: best star of queries lane and lane + 32 over the warp's items
+  uint32_t star0 = COST_INF, star1 = COST_INF;
+  unsigned long long relaxed = 0;
+  uint32_t any = 0;
+  const bool mine = (uint32_t)lane < nsec;
+  const uint32_t s = (uint32_t)lane;
+  for (uint32_t it = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; it < n; it += warps) {
+    const uint2 item = b->items[it];
+    const uint32_t v = item.x, chunk = item.y;
+    uint32_t m = 0;
+    if (mine) m = (__ldcg(&b->am[(uint64_t)v * Wm + (s >> 2)]) >> ((s & 3u) * 8u)) & 0xFFu;
+    uint32_t dv[8], cut[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      dv[i] = COST_INF;
+      cut[i] = mine ? s_cut[s * 8 + i] : 0u;
+    }
+    if (mine && (m || chunk == 0)) {
+      const uint4* src = (const uint4*)&dist[(uint64_t)v * Gp + s * 8];
+      const uint4 a = __ldcg(src), c4 = __ldcg(src + 1);
+      dv[0] = a.x;
+      dv[1] = a.y;
+      dv[2] = a.z;
+      dv[3] = a.w;
+      dv[4] = c4.x;
+      dv[5] = c4.y;
+      dv[6] = c4.z;
+      dv[7] = c4.w;
+    }
+    if (chunk == 0) {
+      // stars of every query at v (v's row in shared memory, one query per lane)
+      if (mine) {
+#pragma unroll
+        for (int i = 0; i < 8; i++) s_row[wib][s * 8 + i] = dv[i];
+      }
+      __syncwarp();
+      for (uint32_t q = (uint32_t)lane; q < nq; q += 32) {
+        uint64_t sum = 0;
+        for (uint32_t i = 0; i < b->qk[q]; i++) sum += s_row[wib][b->qcol[q][i]];
+        if (sum < COST_INF) {
+          if (q < 32) star0 = min(star0, (uint32_t)sum);
+          else star1 = min(star1, (uint32_t)sum);
+        }
+      }
+      __syncwarp();
+    }
+    // the heaviest edge any active column may still take from v
+    uint32_t wl = 0, amask = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+      if (((m >> i) & 1u) && dv[i] < cut[i]) {
+        wl = max(wl, cut[i] - dv[i]);
+        amask |= 1u << i;
+      }
+    wl = __reduce_max_sync(0xffffffffu, wl);
+    const int64_t b0 = G.beg[v], b1 = G.beg[v + 1];
+    const int64_t cnt = count_upto(G, v, b1 - b0, wl);
+    const int64_t e0 = (int64_t)chunk * BS_CHUNK, e1 = min(cnt, e0 + BS_CHUNK);
+    const bool act = amask != 0u;
+    // work: the target-row sectors this item reads, one per active lane and edge
+    const uint32_t nact = (uint32_t)__popc(__ballot_sync(0xffffffffu, act));
+    if (e1 > e0) relaxed += (unsigned long long)(e1 - e0) * nact;
+    int2 ed = e0 < e1 ? G.wedges[b0 + e0] : make_int2(0, 0);
+    for (int64_t e = e0; e < e1; e++) {
+      const uint32_t u = (uint32_t)ed.x, w = (uint32_t)ed.y;
+      uint4 ra = make_uint4(0, 0, 0, 0), rb = ra;
+      const bool go = act && u < G.V;
+      if (go) {
+        const uint4* dst = (const uint4*)&dist[(uint64_t)u * Gp + s * 8];
+        ra = __ldcg(dst);
+        rb = __ldcg(dst + 1);
+      }
+      if (e + 1 < e1) ed = G.wedges[b0 + e + 1];
+      if (go) {
+        const uint32_t du[8] = {ra.x, ra.y, ra.z, ra.w, rb.x, rb.y, rb.z, rb.w};
+        uint32_t imp = 0;
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+          if (((amask >> i) & 1u) && w <= cut[i] - dv[i]) {
+            const uint32_t nd = dv[i] + w;
+            if (nd < du[i]) {
+              atomicMin(&dist[(uint64_t)u * Gp + s * 8 + i], nd);
+              if (nd < cut[i]) imp |= 1u << i;
+            }
+          }
+        }
+        if (imp) {
+          atomicOr(&fo[(uint64_t)u * Wm + (s >> 2)], imp << ((s & 3u) * 8u));
+          any = 1u;
+        }
+      }
+    }
+  }
+  any = __reduce_or_sync(0xffffffffu, any);
+  if (lane == 0 && any) b->ann = 1u;
+  if (star0 < COST_INF && lane < (int)nq) atomicMin(&b->star[lane], star0);
+  if (star1 < COST_INF && lane + 32 < (int)nq) atomicMin(&b->star[lane + 32], star1);
+  if (lane == 0 && relaxed) atomicAdd(&b->st_relax, relaxed);  // the same in every lane
+}
+
+// Control (one block): column cutoffs from the query stars; the next step's buffers; the
+// end of the search.
+__global__ void k_bs_ctrl(BsCtx* b) {
+  if (b->done) return;
+  const uint32_t nq = b->nq, Gp = b->Gp;
+  for (uint32_t c = threadIdx.x; c < Gp; c += blockDim.x) {
+    uint32_t mx = 0;
+    bool used = false;
+    for (uint32_t q = 0; q < nq; q++)
+      for (uint32_t i = 0; i < b->qk[q]; i++)
+        if (b->qcol[q][i] == c) {
+          used = true;
+          const uint32_t st = b->star[q];
+          const uint64_t x = st == COST_INF ? COST_INF : (uint64_t)st * b->cut_pm / 1000u;
+          mx = max(mx, x >= COST_INF ? COST_INF : (uint32_t)x);
+        }
+    if (used) b->cutc[c] = min(b->cutc[c], mx);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (b->error || !b->ann) {
+      b->done = 1u;
+    } else if (++b->steps > b->max_steps) {
+      b->error |= BS_ERR_STEPS;
+      b->done = 1u;
+    } else {
+      b->ann = 0u;
+      b->in ^= 1u;
+      b->n_items = 0u;
+    }
+  }
+}
+
+// A query's distance rows (stride ds) from the shared table: column cols[i] for group i.
+__global__ void k_bs_gather(uint32_t* rows, uint32_t ds, int k, const BsCtx* b, ushort4 c0,
+                            ushort4 c1, int64_t V) {
+  const uint32_t Gp = b->Gp;
+  const uint16_t cols[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < V;
+       v += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t d[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) d[i] = i < k ? __ldcg(&b->dist[(uint64_t)v * Gp + cols[i]]) : COST_INF;
+    store_drow(rows, ds, (uint64_t)v, make_uint4(d[0], d[1], d[2], d[3]), make_uint4(d[4], d[5], d[6], d[7]));
+  }
+}
+
+}  // namespace gst

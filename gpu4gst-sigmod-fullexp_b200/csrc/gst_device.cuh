@@ -193,6 +193,8 @@ struct Ctx {
   uint32_t ub;          // best feasible cost known (one-label solutions and full cells)
   uint32_t cut;         // cutoff when the one-label distances became final: a distance
                         // above it (or unreached) is only known to exceed it
+  uint32_t cut_fix;     // nonzero: the distances came from a batch-shared search, exact up
+                        // to this cutoff (it replaces the star-bound cutoff below)
   uint32_t cut_pm;      // the distance search stops at cut_pm / 1000 x ub: below 1000 it
                         // searches less and leaves weaker (still valid) bounds to the DP;
                         // hop-bounded queries, which prune against their own larger bound,
@@ -359,6 +361,7 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x) {
 // every bound uses min(d, cut + 1).  A lower cutoff trades search work for DP work.
 __device__ __forceinline__ uint32_t sssp_cutoff(const Ctx* c) {
   if (c->sssp_full) return COST_INF;
+  if (c->cut_fix) return c->cut_fix;
   uint32_t ub = __ldcg(&c->ub);
   if (c->sssp_hops) {
     const uint32_t h = __ldcg(&c->ub_hop);

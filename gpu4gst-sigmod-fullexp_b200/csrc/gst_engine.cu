@@ -34,6 +34,7 @@
 
 #include "gst.h"
 #include "gst_device.cuh"
+#include "gst_bsearch.cuh"
 
 using namespace gst;
 
@@ -161,6 +162,7 @@ struct gst_engine {
   std::vector<std::pair<uint64_t, int>> rows_occ;  // (threads<<32 | smem) -> grid
   size_t rows_smem = 0;                            // dynamic shared memory a rows CTA may take
   std::atomic<int> graphs{0};                      // live graphs (the engine outlives them)
+  cudaEvent_t bs_ev[2] = {nullptr, nullptr};       // timing of batch-shared searches
   std::string err;
   std::mutex mu;                                   // serialises all GPU work of the engine
 };
@@ -366,6 +368,11 @@ struct Job {
   uint32_t ds = DIST_STRIDE;     // uint32 per distance row
   uint32_t* cache_dst = nullptr; // a group-cache fill: the distances of group gids[0] to
                                  // every vertex go here (V entries), no DP
+  // batch-shared search: 1 when the runner's shared table holds this query's distances
+  // (its groups in columns ss_cols), exact up to ss_cut
+  int ss = 0;
+  uint16_t ss_cols[KMAX] = {0};
+  uint32_t ss_cut = 0;
   std::atomic<bool> done{false};
 };
 
@@ -375,6 +382,8 @@ struct CallStats {
   int64_t graph_launches = 0, graph_levels = 0;
   int64_t allocs = 0, alloc_bytes = 0;
   double alloc_ms = 0;
+  int64_t bs_sectors = 0, bs_launches = 0;  // batch-shared searches of the call
+  double bs_ms = 0;
   std::vector<std::pair<int, int>> prof;  // (kernel kind, event-pair index)
   size_t next_ev = 0;
 };
@@ -416,6 +425,14 @@ struct Runner {
     cudaGraphExec_t exec = nullptr;
   };
   std::vector<LoopGraph> graphs;
+  // Batch-shared distance search (gst_bsearch.cuh): its table lives in the arenas until
+  // every query of its chunk has been admitted (and gathered its columns).
+  struct Shared {
+    void* mem = nullptr;
+    size_t bytes = 0;
+    BsCtx* d_b = nullptr;
+    int remaining = 0;
+  } sh;
 
   Runner(gst_engine* e, gst_graph* gr, int slots) : eng(e), g(gr), max_slots(slots) {}
   ~Runner() { release(); }
@@ -428,6 +445,7 @@ struct Runner {
       if (lg.graph) cudaGraphDestroy(lg.graph);
     }
     graphs.clear();
+    sh = Shared();  // its memory is one of the arenas' ranges
     for (auto& a : arenas) cudaFreeAsync(a.base, eng->stream);
     cudaStreamSynchronize(eng->stream);
     arenas.clear();
@@ -678,7 +696,15 @@ struct Runner {
       for (int i = 0; i < q->k; i++) n_cached += (hv[i] = grp->hop_cache.vec(c.gid[i])) != nullptr;
       for (int i = 0; i < q->k; i++) gv.v[i] = hv[i] ? hv[i] + (size_t)c.nhb * V : nullptr;
     }
-    const bool cached = n_cached > 0;
+    // a query of the batch-shared search: its distances are in the runner's shared
+    // table, exact up to its cutoff; it starts at the bounds pass
+    const bool shared = j->ss == 1 && sh.d_b != nullptr && !hop;
+    if (shared) {
+      n_cached = 0;
+      c.cut_fix = std::max(1u, j->ss_cut);
+      c.phase = PH_PREP;
+    }
+    const bool cached = n_cached > 0 || shared;
     if (n_cached == q->k) {
       c.sssp_full = 1;
       c.phase = PH_PREP;
@@ -702,7 +728,14 @@ struct Runner {
     CK(cudaMemcpyAsync(d_ctx + s, &c, sizeof(Ctx), cudaMemcpyHostToDevice, st));
     cs.h2d += sizeof(Ctx) + sizeof(int32_t) * q->k;
     const DevGraph G = dev_graph(g);
-    if (cached) {
+    if (shared) {
+      const uint16_t* sc = j->ss_cols;
+      k_bs_gather<<<eng->sssp_blocks, 256, 0, st>>>(m.dist, c.ds, q->k, sh.d_b,
+                                                    make_ushort4(sc[0], sc[1], sc[2], sc[3]),
+                                                    make_ushort4(sc[4], sc[5], sc[6], sc[7]), g->V);
+      cs.launches += 1;
+      sh.remaining--;
+    } else if (cached) {
       k_gather_dist<<<eng->sssp_blocks, 256, 0, st>>>(m.dist, c.ds, q->k, gv, g->V);
       cs.launches += 1;
       if (hop)
@@ -716,7 +749,7 @@ struct Runner {
     }
     k_init<<<dim3(64, 1), 256, 0, st>>>(d_ctx + s, 1, G, grp->d_ptr, grp->d_mem,
                                        eng->cfg.split_degree);
-    if (n_cached == q->k) {
+    if (n_cached == q->k || shared) {
       // the bounds pass over the distance rows (star bound, group distances), which
       // the control step after it turns into the tour table
       k_sssp<<<eng->sssp_blocks, 256, 0, st>>>(d_ctx + s, 1, G, eng->cfg.split_degree);
@@ -728,6 +761,122 @@ struct Runner {
     idle_written[s] = 0;
     nctx = std::max(nctx, s + 1);
     active++;
+    return GST_OK;
+  }
+
+  // Give back the shared table once every query of its chunk has been admitted.
+  void shared_release() {
+    if (sh.mem) arena_give(sh.mem, sh.bytes);
+    sh = Shared();
+  }
+
+  // One batch-shared distance search for the unbounded queries `jobs` over their distinct
+  // groups `cols` (at most BS_COLS groups, BS_MAXQ queries).  On success every job is
+  // marked (ss = 1) with its columns and cutoff; without memory for the table, or when
+  // the search reports an error, the jobs keep their own searches.
+  gst_status shared_search(const std::vector<Job*>& jobs, const std::vector<int32_t>& cols) {
+    const int64_t V = g->V;
+    const uint32_t ncols = (uint32_t)cols.size();
+    const uint32_t Gp = (ncols + 7u) / 8u * 8u, Wm = (Gp + 31u) / 32u;
+    const uint64_t item_cap = (uint64_t)V + (uint64_t)g->E / BS_CHUNK + 1024;
+    if (item_cap >= (1ull << 32)) return GST_OK;
+    size_t off = 0;
+    auto take = [&](size_t n) {
+      const size_t o = off;
+      off = align256(off + n);
+      return o;
+    };
+    const size_t o_b = take(sizeof(BsCtx));
+    const size_t o_dist = take((size_t)V * Gp * 4);
+    const size_t o_fm0 = take((size_t)V * Wm * 4);
+    const size_t o_fm1 = take((size_t)V * Wm * 4);
+    const size_t o_am = take((size_t)V * Wm * 4);
+    const size_t o_items = take((size_t)item_cap * 8);
+    const size_t o_cols = take((size_t)BS_COLS * 4);
+    void* p = nullptr;
+    gst_status s = slot_memory(off, &p);
+    if (s != GST_OK) return s;
+    if (!p) return GST_OK;  // no room: the queries search on their own
+    unsigned char* base = (unsigned char*)p;
+    sh.mem = p;
+    sh.bytes = off;
+    BsCtx h;
+    memset(&h, 0, sizeof(h));
+    h.dist = (uint32_t*)(base + o_dist);
+    h.fm[0] = (uint32_t*)(base + o_fm0);
+    h.fm[1] = (uint32_t*)(base + o_fm1);
+    h.am = (uint32_t*)(base + o_am);
+    h.items = (uint2*)(base + o_items);
+    h.item_cap = (uint32_t)item_cap;
+    h.Gp = Gp;
+    h.Wm = Wm;
+    h.max_steps = (uint32_t)std::min(eng->cfg.max_levels, 1 << 16);
+    h.cut_pm = (uint32_t)(eng->cfg.search_cut_permille > 0 ? eng->cfg.search_cut_permille : 1000);
+    h.nq = (uint32_t)jobs.size();
+    for (size_t q = 0; q < jobs.size(); q++) {
+      h.qk[q] = (uint32_t)jobs[q]->q.k;
+      h.star[q] = COST_INF;
+      for (int i = 0; i < jobs[q]->q.k; i++)
+        h.qcol[q][i] =
+            (uint16_t)(std::find(cols.begin(), cols.end(), jobs[q]->gids[i]) - cols.begin());
+    }
+    for (int c = 0; c < BS_COLS; c++) h.cutc[c] = COST_INF;
+    cudaStream_t st = eng->stream;
+    BsCtx* d_b = (BsCtx*)(base + o_b);
+    int32_t* d_cols = (int32_t*)(base + o_cols);
+    if (!eng->bs_ev[0]) {
+      CK(cudaEventCreate(&eng->bs_ev[0]));
+      CK(cudaEventCreate(&eng->bs_ev[1]));
+    }
+    CK(cudaEventRecord(eng->bs_ev[0], st));
+    CK(cudaMemsetAsync(h.dist, 0xFF, (size_t)V * Gp * 4, st));
+    CK(cudaMemsetAsync(h.fm[0], 0, (size_t)V * Wm * 4, st));
+    CK(cudaMemsetAsync(h.fm[1], 0, (size_t)V * Wm * 4, st));
+    CK(cudaMemcpyAsync(d_b, &h, sizeof(BsCtx), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_cols, cols.data(), ncols * 4, cudaMemcpyHostToDevice, st));
+    cs.h2d += sizeof(BsCtx) + ncols * 4;
+    const DevGraph G = dev_graph(g);
+    k_bs_seed<<<dim3(16, ncols), 256, 0, st>>>(d_b, G, grp->d_ptr, grp->d_mem, d_cols, (int)ncols);
+    int64_t launches = 1;
+    int occ = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_bs_relax, 256, 0);
+    const int relax_blocks = eng->sms * std::max(1, std::min(occ, 4));
+    BsCtx hb;
+    for (;;) {
+      for (int i = 0; i < 6; i++) {
+        k_bs_scan<<<eng->sms * 4, 256, 0, st>>>(d_b, G);
+        k_bs_relax<<<relax_blocks, 256, 0, st>>>(d_b, G);
+        k_bs_ctrl<<<1, 256, 0, st>>>(d_b);
+        launches += 3;
+      }
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(&hb, d_b, sizeof(BsCtx), cudaMemcpyDeviceToHost, st));
+      cs.d2h += sizeof(BsCtx);
+      CK(cudaStreamSynchronize(st));
+      if (hb.done) break;
+    }
+    CK(cudaEventRecord(eng->bs_ev[1], st));
+    CK(cudaEventSynchronize(eng->bs_ev[1]));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, eng->bs_ev[0], eng->bs_ev[1]);
+    cs.bs_ms += ms;
+    cs.bs_sectors += (int64_t)hb.st_relax;
+    cs.bs_launches += launches;
+    cs.launches += launches;
+    sh.d_b = d_b;
+    if (hb.error) {  // the queries search on their own
+      shared_release();
+      return GST_OK;
+    }
+    // a query's cutoff: the smallest final cutoff of its columns
+    for (size_t q = 0; q < jobs.size(); q++) {
+      uint32_t cut = COST_INF;
+      for (int i = 0; i < jobs[q]->q.k; i++) cut = std::min(cut, hb.cutc[hb.qcol[q][i]]);
+      for (int i = 0; i < KMAX; i++) jobs[q]->ss_cols[i] = i < jobs[q]->q.k ? hb.qcol[q][i] : 0;
+      jobs[q]->ss_cut = cut;
+      jobs[q]->ss = 1;
+    }
+    sh.remaining = (int)jobs.size();
     return GST_OK;
   }
 
@@ -923,6 +1072,7 @@ struct Runner {
       const bool pool_full = (c.error & ERR_POOL) && c.rowmap != nullptr;
       if (list_full || pool_full) {
         j->boost++;
+        j->ss = 0;  // a retry searches on its own
         retry.push_back(j);
         continue;
       }
@@ -1170,6 +1320,7 @@ void gst_config_default(gst_config* cfg) {
   cfg->verbose = 0;
   cfg->hop_cut_mult = 1;
   cfg->search_cut_permille = 1000;
+  cfg->batch_search = 1;
 }
 
 gst_status gst_engine_create(int32_t device, const gst_config* cfg, gst_engine** out) {
@@ -1241,6 +1392,8 @@ gst_status gst_engine_destroy(gst_engine* eng) {
     cudaStreamDestroy(eng->stream);
   }
   for (auto e : eng->prof_events) cudaEventDestroy(e);
+  for (auto e : eng->bs_ev)
+    if (e) cudaEventDestroy(e);
   if (eng->pool) cudaMemPoolDestroy(eng->pool);
   delete eng;
   return GST_OK;
@@ -1446,6 +1599,37 @@ namespace {
 // would change it), refilling slots as queries finish; capacity overflows are re-run
 // with more room.  A job that does not fit the free memory yet does not hold back the
 // smaller ones behind it (a batch has no arrival order to keep).
+// A query the batch-shared search may serve: unbounded, a first attempt, not a cache
+// fill, none of its groups in the group cache (those start from exact distances).
+bool shared_eligible(const Runner& R, const Job* j) {
+  if (j->q.hop_bound >= 0 || j->cache_dst || j->boost > 0 || j->ss) return false;
+  for (int i = 0; i < j->q.k; i++)
+    if (R.grp->cache.vec(j->gids[i])) return false;
+  return true;
+}
+
+// Before admitting: when no shared table is pending and at least two eligible queries
+// wait, search their groups together (the first eligible queries in order, up to
+// BS_COLS distinct groups and BS_MAXQ queries).
+gst_status maybe_shared_search(Runner& R, std::deque<Job*>& pending) {
+  if (!R.eng->cfg.batch_search || R.sh.remaining > 0) return GST_OK;
+  if (R.sh.mem) R.shared_release();
+  std::vector<Job*> chunk;
+  std::vector<int32_t> cols;
+  for (Job* j : pending) {
+    if (!shared_eligible(R, j)) continue;
+    int add = 0;
+    for (int i = 0; i < j->q.k; i++)
+      add += std::find(cols.begin(), cols.end(), j->gids[i]) == cols.end();
+    if ((int)cols.size() + add > BS_COLS || (int)chunk.size() >= BS_MAXQ) break;
+    for (int i = 0; i < j->q.k; i++)
+      if (std::find(cols.begin(), cols.end(), j->gids[i]) == cols.end()) cols.push_back(j->gids[i]);
+    chunk.push_back(j);
+  }
+  if (chunk.size() < 2) return GST_OK;
+  return R.shared_search(chunk, cols);
+}
+
 gst_status drive(Runner& R, std::deque<Job*>& pending, int B) {
   gst_engine* eng = R.eng;
   const int saved = R.max_slots;
@@ -1453,6 +1637,8 @@ gst_status drive(Runner& R, std::deque<Job*>& pending, int B) {
   gst_status st = GST_OK;
   std::vector<Job*> done, retry;
   while (st == GST_OK && (!pending.empty() || R.active > 0)) {
+    st = maybe_shared_search(R, pending);
+    if (st != GST_OK) break;
     for (auto it = pending.begin(); it != pending.end() && R.active < R.max_slots;) {
       gst_status s = R.admit(*it);
       if (s == GST_NOT_READY) {
@@ -1461,6 +1647,7 @@ gst_status drive(Runner& R, std::deque<Job*>& pending, int B) {
       }
       if (s == GST_OOM_ADMISSION) {
         Job* j = *it;
+        if (j->ss == 1) R.sh.remaining--;  // never gathers its columns
         j->out->status = GST_OOM_ADMISSION;
         j->out->user_tag = j->q.user_tag;
         fail(eng, GST_OOM_ADMISSION, "solve: the query's state table does not fit the memory budget");
@@ -1477,6 +1664,7 @@ gst_status drive(Runner& R, std::deque<Job*>& pending, int B) {
     if (st == GST_OK) st = R.harvest(done, retry);
     for (Job* j : retry) pending.push_front(j);
   }
+  R.shared_release();
   R.max_slots = saved;
   return st;
 }
@@ -1683,6 +1871,9 @@ gst_status gst_solve_batch(gst_graph* g, gst_groups* grp, int32_t n, const gst_q
     s.grow_launches = kn[PROF_GROW];
     s.rows_launches = kn[PROF_ROWS];
     s.sssp_launches = kn[PROF_SSSP];
+    s.shared_sectors = R.cs.bs_sectors;
+    s.shared_ms = R.cs.bs_ms;
+    s.shared_launches = R.cs.bs_launches;
   }
   return GST_OK;
 }
@@ -1760,7 +1951,8 @@ std::string shape_key(const gst_graph* g, int32_t max_batch) {
 }
 
 struct TuneParams {
-  int32_t split_degree, bucket_delta, threads_per_block, blocks_per_sm, max_batch, search_cut;
+  int32_t split_degree, bucket_delta, threads_per_block, blocks_per_sm, max_batch, search_cut,
+      batch_search;
 };
 
 void set_params(gst_graph* g, const TuneParams& p) {
@@ -1771,6 +1963,7 @@ void set_params(gst_graph* g, const TuneParams& p) {
   eng->cfg.blocks_per_sm = p.blocks_per_sm;
   eng->cfg.max_batch = std::max(1, std::min(MAXB, p.max_batch));
   eng->cfg.search_cut_permille = std::max(1, p.search_cut);
+  eng->cfg.batch_search = p.batch_search ? 1 : 0;
   apply_launch_config(eng);
   g->batch.reset();  // its CUDA graphs hold the old launch geometry
 }
@@ -1787,8 +1980,9 @@ bool read_cache(const char* path, const std::string& key, TuneParams* p) {
     *bar = 0;
     if (key != line) continue;
     TuneParams t;
-    if (sscanf(bar + 1, "%d %d %d %d %d %d", &t.split_degree, &t.bucket_delta, &t.threads_per_block,
-               &t.blocks_per_sm, &t.max_batch, &t.search_cut) == 6) {
+    if (sscanf(bar + 1, "%d %d %d %d %d %d %d", &t.split_degree, &t.bucket_delta,
+               &t.threads_per_block, &t.blocks_per_sm, &t.max_batch, &t.search_cut,
+               &t.batch_search) == 7) {
       *p = t;
       hit = true;  // the last line for a key wins
     }
@@ -1807,7 +2001,8 @@ extern "C" gst_status gst_autotune(gst_graph* g, gst_groups* grp, int32_t n,
     return fail(eng, GST_BAD_INPUT, "autotune: bad arguments");
   const std::string key = shape_key(g, eng->cfg.max_batch);
   TuneParams cur{eng->cfg.split_degree, eng->cfg.bucket_delta, eng->cfg.threads_per_block,
-                 eng->cfg.blocks_per_sm, eng->cfg.max_batch, eng->cfg.search_cut_permille};
+                 eng->cfg.blocks_per_sm, eng->cfg.max_batch, eng->cfg.search_cut_permille,
+                 eng->cfg.batch_search};
   TuneParams hit;
   if (read_cache(cache_path, key, &hit)) {
     std::lock_guard<std::mutex> lk(eng->mu);
@@ -1858,20 +2053,23 @@ extern "C" gst_status gst_autotune(gst_graph* g, gst_groups* grp, int32_t n,
   for (int32_t b : {1, 2, 4, 8, 16, 32, 64})
     if (b < cur.max_batch) c_batch.push_back(b);
   const std::vector<int32_t> c_cut = {1000, 875, 750};  // search cutoff, permille of ub
-  for (int param = 0; param < 6 && st == GST_OK; param++) {
-    const std::vector<int32_t>& cand = param == 0   ? c_cut
-                                       : param == 1 ? c_split
-                                       : param == 2 ? c_delta
-                                       : param == 3 ? c_tpb
-                                       : param == 4 ? c_bps
+  const std::vector<int32_t> c_bsearch = {1, 0};  // batch-shared distance search
+  for (int param = 0; param < 7 && st == GST_OK; param++) {
+    const std::vector<int32_t>& cand = param == 0   ? c_bsearch
+                                       : param == 1 ? c_cut
+                                       : param == 2 ? c_split
+                                       : param == 3 ? c_delta
+                                       : param == 4 ? c_tpb
+                                       : param == 5 ? c_bps
                                                     : c_batch;
     for (int32_t v : cand) {
       TuneParams p = cur;
-      int32_t* field = param == 0   ? &p.search_cut
-                       : param == 1 ? &p.split_degree
-                       : param == 2 ? &p.bucket_delta
-                       : param == 3 ? &p.threads_per_block
-                       : param == 4 ? &p.blocks_per_sm
+      int32_t* field = param == 0   ? &p.batch_search
+                       : param == 1 ? &p.search_cut
+                       : param == 2 ? &p.split_degree
+                       : param == 3 ? &p.bucket_delta
+                       : param == 4 ? &p.threads_per_block
+                       : param == 5 ? &p.blocks_per_sm
                                     : &p.max_batch;
       if (*field == v) continue;
       *field = v;
@@ -1893,8 +2091,9 @@ extern "C" gst_status gst_autotune(gst_graph* g, gst_groups* grp, int32_t n,
   if (cache_path) {
     FILE* f = fopen(cache_path, "a");
     if (f) {
-      fprintf(f, "%s|%d %d %d %d %d %d\n", key.c_str(), cur.split_degree, cur.bucket_delta,
-              cur.threads_per_block, cur.blocks_per_sm, cur.max_batch, cur.search_cut);
+      fprintf(f, "%s|%d %d %d %d %d %d %d\n", key.c_str(), cur.split_degree, cur.bucket_delta,
+              cur.threads_per_block, cur.blocks_per_sm, cur.max_batch, cur.search_cut,
+              cur.batch_search);
       fclose(f);
     }
   }

@@ -274,7 +274,7 @@ class Config(C.Structure):
                 ("max_batch", C.c_int32), ("use_graphs", C.c_int32),
                 ("profile_kernels", C.c_int32), ("verbose", C.c_int32),
                 ("hop_cut_mult", C.c_int32), ("search_cut_permille", C.c_int32),
-                ("hop_cut_permille", C.c_int32)]
+                ("hop_cut_permille", C.c_int32), ("batch_search", C.c_int32)]
 
 
 class Query(C.Structure):
@@ -290,7 +290,9 @@ class Stats(C.Structure):
                 ("d2h_bytes", C.c_int64), ("device_ms", C.c_double), ("latency_ms", C.c_double),
                 ("grow_ms", C.c_double), ("rows_ms", C.c_double), ("sssp_ms", C.c_double),
                 ("queue_max", C.c_int64), ("grow_launches", C.c_int64),
-                ("rows_launches", C.c_int64), ("sssp_launches", C.c_int64)]
+                ("rows_launches", C.c_int64), ("sssp_launches", C.c_int64),
+                ("shared_sectors", C.c_int64), ("shared_ms", C.c_double),
+                ("shared_launches", C.c_int64)]
 
 
 class Result(C.Structure):

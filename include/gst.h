@@ -80,6 +80,10 @@ typedef struct gst_config {
                                  bounds to the DP (the autotuner chooses it) */
   int32_t hop_cut_permille;   /* hop-bounded queries: the same in thousandths (0: use
                                  hop_cut_mult x 1000) */
+  int32_t batch_search;       /* 1 (default): gst_solve_batch searches the distances of its
+                                 unbounded queries' groups together, up to 256 groups at a
+                                 time (one relaxation of an edge serves every group that
+                                 improved at its source); 0: every query searches alone */
 } gst_config;
 
 typedef struct gst_query {
@@ -108,6 +112,10 @@ typedef struct gst_stats {
   int64_t grow_launches;    /* profiled launches behind grow_ms / rows_ms / sssp_ms */
   int64_t rows_launches;
   int64_t sssp_launches;
+  int64_t shared_sectors;   /* batch-shared distance search of the call: target-row sectors
+                               read (edges x active 8-group sectors), */
+  double shared_ms;         /*   its device time, */
+  int64_t shared_launches;  /*   and its kernel launches */
 } gst_stats;
 
 typedef struct gst_result {
