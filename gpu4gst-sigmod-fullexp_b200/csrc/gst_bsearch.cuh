@@ -19,6 +19,17 @@
 // final cutoff of its columns as its own `cut` (distances above it are clamped to cut + 1
 // by every bound), at least as strong as its own search would have reached.
 //
+// Hop-bounded queries of one bound D (1 <= D <= KMAX) share a search the same way over
+// D tables: table h holds d^{<=h}, the cheapest paths of at most h edges (table D is the
+// distance table, 1..D-1 the hop budgets).  One step is one round: round r (r >= 1)
+// first copies table r into table r+1 (a coalesced pass, so that table r+1 starts from
+// the paths of at most r edges), then relaxes the edges of the vertices whose table r
+// row improved in round r-1 (round 0: the members, distance 0) from table r into table
+// r+1 alone.  Table r is final while round r reads it, so no snapshot is needed, and
+// the result is the per-query rounds'.  Stars come from tables r with 2r <= D (trees of
+// diameter <= D), as in the per-query search; after the last round the tables above
+// it are filled from it.
+//
 // Per step: k_bs_scan turns the announcement bits of the previous step into relax items
 // of at most BS_CHUNK edges (a hub's range spread over many warps), k_bs_relax relaxes
 // them, k_bs_ctrl updates the cutoffs and ends the search when nothing was announced.
@@ -43,6 +54,9 @@ struct BsCtx {
   uint32_t ann;         // the relax step announced something
   uint32_t done, steps, max_steps, error;
   uint32_t cut_pm;      // query cutoff: star x cut_pm / 1000
+  uint32_t D;           // 0: unbounded distances; else the hop bound (rounds 0..D-1)
+  uint32_t round;       // hop-bounded: the current round
+  uint32_t* tab[KMAX + 1];  // hop-bounded: tab[h] = d^{<=h} (V x Gp), tab[D] = dist
   uint32_t nq;          // queries
   uint32_t qk[BS_MAXQ];
   uint16_t qcol[BS_MAXQ][KMAX];  // columns of each query's groups
@@ -63,7 +77,7 @@ __global__ void k_bs_seed(BsCtx* b, DevGraph G, const int64_t* grp_ptr, const in
        j += (int64_t)gridDim.x * blockDim.x) {
     const uint32_t v = (uint32_t)members[j];
     if (v >= G.V) continue;
-    atomicMin(&b->dist[(uint64_t)v * Gp + c], 0u);
+    atomicMin(&(b->D ? b->tab[1] : b->dist)[(uint64_t)v * Gp + c], 0u);
     if (G.beg[v + 1] > G.beg[v]) atomicOr(&b->fm[b->in][(uint64_t)v * Wm + (c >> 5)], 1u << (c & 31));
   }
 }
@@ -130,8 +144,16 @@ __global__ void __launch_bounds__(256, 4) k_bs_relax(BsCtx* b, DevGraph G) {
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const uint32_t n = min(b->n_items, b->item_cap);
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-  uint32_t* dist = b->dist;
   uint32_t* fo = b->fm[b->in ^ 1u];
+  // hop-bounded round r: sources in table r (the members at 0 for r = 0), targets in
+  // table r + 1; a round's paths extend only while they have fewer than D edges; stars
+  // from tables r with 2r <= D
+  const uint32_t D = b->D, r = b->round;
+  if (D && r >= D) return;
+  const uint32_t* src_tab = D ? (r ? b->tab[r] : nullptr) : b->dist;
+  uint32_t* dst_tab = D ? b->tab[r + 1] : b->dist;
+  const bool extend = D == 0u || r + 1u < D;
+  const bool stars = D == 0u || (r >= 1u && 2u * r <= D);
   // per lane: best star of queries lane and lane + 32 over the warp's items
   uint32_t star0 = COST_INF, star1 = COST_INF;
   unsigned long long relaxed = 0;
@@ -149,8 +171,12 @@ __global__ void __launch_bounds__(256, 4) k_bs_relax(BsCtx* b, DevGraph G) {
       dv[i] = COST_INF;
       cut[i] = mine ? s_cut[s * 8 + i] : 0u;
     }
-    if (mine && (m || chunk == 0)) {
-      const uint4* src = (const uint4*)&dist[(uint64_t)v * Gp + s * 8];
+    if (mine && !src_tab) {
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+        if ((m >> i) & 1u) dv[i] = 0u;  // round 0: the members themselves
+    } else if (mine && (m || (chunk == 0 && stars))) {
+      const uint4* src = (const uint4*)&src_tab[(uint64_t)v * Gp + s * 8];
       const uint4 a = __ldcg(src), c4 = __ldcg(src + 1);
       dv[0] = a.x;
       dv[1] = a.y;
@@ -161,7 +187,7 @@ __global__ void __launch_bounds__(256, 4) k_bs_relax(BsCtx* b, DevGraph G) {
       dv[6] = c4.z;
       dv[7] = c4.w;
     }
-    if (chunk == 0) {
+    if (chunk == 0 && stars) {
       // stars of every query at v (v's row in shared memory, one query per lane)
       if (mine) {
 #pragma unroll
@@ -200,7 +226,7 @@ __global__ void __launch_bounds__(256, 4) k_bs_relax(BsCtx* b, DevGraph G) {
       uint4 ra = make_uint4(0, 0, 0, 0), rb = ra;
       const bool go = act && u < G.V;
       if (go) {
-        const uint4* dst = (const uint4*)&dist[(uint64_t)u * Gp + s * 8];
+        const uint4* dst = (const uint4*)&dst_tab[(uint64_t)u * Gp + s * 8];
         ra = __ldcg(dst);
         rb = __ldcg(dst + 1);
       }
@@ -213,8 +239,8 @@ __global__ void __launch_bounds__(256, 4) k_bs_relax(BsCtx* b, DevGraph G) {
           if (((amask >> i) & 1u) && w <= cut[i] - dv[i]) {
             const uint32_t nd = dv[i] + w;
             if (nd < du[i]) {
-              atomicMin(&dist[(uint64_t)u * Gp + s * 8 + i], nd);
-              if (nd < cut[i]) imp |= 1u << i;
+              atomicMin(&dst_tab[(uint64_t)u * Gp + s * 8 + i], nd);
+              if (nd < cut[i] && extend) imp |= 1u << i;
             }
           }
         }
@@ -230,6 +256,31 @@ __global__ void __launch_bounds__(256, 4) k_bs_relax(BsCtx* b, DevGraph G) {
   if (star0 < COST_INF && lane < (int)nq) atomicMin(&b->star[lane], star0);
   if (star1 < COST_INF && lane + 32 < (int)nq) atomicMin(&b->star[lane + 32], star1);
   if (lane == 0 && relaxed) atomicAdd(&b->st_relax, relaxed);  // the same in every lane
+}
+
+// Hop-bounded tables (n4 = V x Gp / 4 uint4 per table).  Before round r >= 1:
+// table r + 1 := table r.  With `finish`, after the search: every table above the last
+// round's target := that target (the search ended early; no path has more edges).
+__global__ void k_bs_copy(BsCtx* b, int64_t n4, int finish) {
+  const uint32_t D = b->D;
+  if (!D) return;
+  uint32_t from, h1;  // tables from + 1..h1 := table from
+  if (!finish) {
+    if (b->done || b->round == 0u || b->round >= D) return;
+    from = b->round;
+    h1 = from + 1u;
+  } else {
+    if (b->error) return;
+    from = b->round + 1u;
+    h1 = D;
+  }
+  if (from >= h1) return;
+  const uint4* src = (const uint4*)b->tab[from];
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n4;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const uint4 x = __ldcs(src + i);
+    for (uint32_t h = from + 1u; h <= h1; h++) __stcs((uint4*)b->tab[h] + i, x);
+  }
 }
 
 // Control (one block): column cutoffs from the query stars; the next step's buffers; the
@@ -261,20 +312,21 @@ __global__ void k_bs_ctrl(BsCtx* b) {
       b->ann = 0u;
       b->in ^= 1u;
       b->n_items = 0u;
+      b->round++;
     }
   }
 }
 
-// A query's distance rows (stride ds) from the shared table: column cols[i] for group i.
-__global__ void k_bs_gather(uint32_t* rows, uint32_t ds, int k, const BsCtx* b, ushort4 c0,
-                            ushort4 c1, int64_t V) {
-  const uint32_t Gp = b->Gp;
+// A query's distance rows (stride ds) from a shared table (V x Gp): column cols[i] for
+// group i.
+__global__ void k_bs_gather(uint32_t* rows, uint32_t ds, int k, const uint32_t* table, uint32_t Gp,
+                            ushort4 c0, ushort4 c1, int64_t V) {
   const uint16_t cols[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
   for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < V;
        v += (int64_t)gridDim.x * blockDim.x) {
     uint32_t d[8];
 #pragma unroll
-    for (int i = 0; i < 8; i++) d[i] = i < k ? __ldcg(&b->dist[(uint64_t)v * Gp + cols[i]]) : COST_INF;
+    for (int i = 0; i < 8; i++) d[i] = i < k ? __ldcg(&table[(uint64_t)v * Gp + cols[i]]) : COST_INF;
     store_drow(rows, ds, (uint64_t)v, make_uint4(d[0], d[1], d[2], d[3]), make_uint4(d[4], d[5], d[6], d[7]));
   }
 }

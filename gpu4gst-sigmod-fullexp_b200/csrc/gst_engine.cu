@@ -368,8 +368,9 @@ struct Job {
   uint32_t ds = DIST_STRIDE;     // uint32 per distance row
   uint32_t* cache_dst = nullptr; // a group-cache fill: the distances of group gids[0] to
                                  // every vertex go here (V entries), no DP
-  // batch-shared search: 1 when the runner's shared table holds this query's distances
-  // (its groups in columns ss_cols), exact up to ss_cut
+  // batch-shared search: 1 when a shared table of the runner holds this query's distances
+  // (its groups in columns ss_cols), exact up to ss_cut; 2 when its table was given back
+  // before it was admitted (it searches on its own)
   int ss = 0;
   uint16_t ss_cols[KMAX] = {0};
   uint32_t ss_cut = 0;
@@ -432,7 +433,17 @@ struct Runner {
     size_t bytes = 0;
     BsCtx* d_b = nullptr;
     int remaining = 0;
-  } sh;
+    int D = 0;                       // 0: unbounded distances; else the hop bound
+    uint32_t Gp = 0;                 // columns of the tables
+    uint32_t* tab[KMAX + 1] = {};    // hop-bounded: d^{<=h} tables (device); tab[D] = dist
+    uint32_t* dist = nullptr;        // the distance table (device)
+  };
+  std::vector<Shared> shs;           // pending shared tables, at most one per kind (D)
+  Shared* shared_of(int D) {
+    for (Shared& x : shs)
+      if (x.D == D && x.d_b) return &x;
+    return nullptr;
+  }
 
   Runner(gst_engine* e, gst_graph* gr, int slots) : eng(e), g(gr), max_slots(slots) {}
   ~Runner() { release(); }
@@ -445,7 +456,7 @@ struct Runner {
       if (lg.graph) cudaGraphDestroy(lg.graph);
     }
     graphs.clear();
-    sh = Shared();  // its memory is one of the arenas' ranges
+    shs.clear();  // their memory is in the arenas
     for (auto& a : arenas) cudaFreeAsync(a.base, eng->stream);
     cudaStreamSynchronize(eng->stream);
     arenas.clear();
@@ -698,7 +709,8 @@ struct Runner {
     }
     // a query of the batch-shared search: its distances are in the runner's shared
     // table, exact up to its cutoff; it starts at the bounds pass
-    const bool shared = j->ss == 1 && sh.d_b != nullptr && !hop;
+    Shared* S = j->ss == 1 ? shared_of(hop ? q->hop_bound : 0) : nullptr;
+    const bool shared = S != nullptr;
     if (shared) {
       n_cached = 0;
       c.cut_fix = std::max(1u, j->ss_cut);
@@ -729,12 +741,18 @@ struct Runner {
     cs.h2d += sizeof(Ctx) + sizeof(int32_t) * q->k;
     const DevGraph G = dev_graph(g);
     if (shared) {
+      // the distance table, and for a hop-bounded query its budgets 1..nhb
       const uint16_t* sc = j->ss_cols;
-      k_bs_gather<<<eng->sssp_blocks, 256, 0, st>>>(m.dist, c.ds, q->k, sh.d_b,
-                                                    make_ushort4(sc[0], sc[1], sc[2], sc[3]),
-                                                    make_ushort4(sc[4], sc[5], sc[6], sc[7]), g->V);
+      const ushort4 c0 = make_ushort4(sc[0], sc[1], sc[2], sc[3]);
+      const ushort4 c1 = make_ushort4(sc[4], sc[5], sc[6], sc[7]);
+      k_bs_gather<<<eng->sssp_blocks, 256, 0, st>>>(m.dist, c.ds, q->k, S->dist, S->Gp, c0, c1, g->V);
       cs.launches += 1;
-      sh.remaining--;
+      for (int h = 1; h <= c.nhb; h++) {
+        k_bs_gather<<<eng->sssp_blocks, 256, 0, st>>>(m.dist_h + (size_t)(h - 1) * V * c.ds, c.ds,
+                                                      q->k, S->tab[h], S->Gp, c0, c1, g->V);
+        cs.launches += 1;
+      }
+      S->remaining--;
     } else if (cached) {
       k_gather_dist<<<eng->sssp_blocks, 256, 0, st>>>(m.dist, c.ds, q->k, gv, g->V);
       cs.launches += 1;
@@ -764,20 +782,29 @@ struct Runner {
     return GST_OK;
   }
 
-  // Give back the shared table once every query of its chunk has been admitted.
-  void shared_release() {
-    if (sh.mem) arena_give(sh.mem, sh.bytes);
-    sh = Shared();
+  // Give back the shared tables whose queries have all been admitted (all of them with
+  // `all`).
+  void shared_release(bool all) {
+    for (size_t i = 0; i < shs.size();) {
+      if (all || shs[i].remaining <= 0) {
+        if (shs[i].mem) arena_give(shs[i].mem, shs[i].bytes);
+        shs.erase(shs.begin() + (std::ptrdiff_t)i);
+      } else {
+        i++;
+      }
+    }
   }
 
-  // One batch-shared distance search for the unbounded queries `jobs` over their distinct
-  // groups `cols` (at most BS_COLS groups, BS_MAXQ queries).  On success every job is
-  // marked (ss = 1) with its columns and cutoff; without memory for the table, or when
-  // the search reports an error, the jobs keep their own searches.
-  gst_status shared_search(const std::vector<Job*>& jobs, const std::vector<int32_t>& cols) {
+  // One batch-shared distance search for the queries `jobs`, all unbounded (D = 0) or all
+  // of hop bound D (1..KMAX), over their distinct groups `cols` (at most BS_COLS groups,
+  // BS_MAXQ queries).  On success every job is marked (ss = 1) with its columns and
+  // cutoff; without memory for the tables, or when the search reports an error, the jobs
+  // keep their own searches.
+  gst_status shared_search(const std::vector<Job*>& jobs, const std::vector<int32_t>& cols, int D) {
     const int64_t V = g->V;
     const uint32_t ncols = (uint32_t)cols.size();
     const uint32_t Gp = (ncols + 7u) / 8u * 8u, Wm = (Gp + 31u) / 32u;
+    if (D < 0 || D > KMAX) return GST_OK;
     const uint64_t item_cap = (uint64_t)V + (uint64_t)g->E / BS_CHUNK + 1024;
     if (item_cap >= (1ull << 32)) return GST_OK;
     size_t off = 0;
@@ -787,7 +814,7 @@ struct Runner {
       return o;
     };
     const size_t o_b = take(sizeof(BsCtx));
-    const size_t o_dist = take((size_t)V * Gp * 4);
+    const size_t o_dist = take((size_t)V * Gp * 4 * (size_t)std::max(D, 1));  // tables 1..D
     const size_t o_fm0 = take((size_t)V * Wm * 4);
     const size_t o_fm1 = take((size_t)V * Wm * 4);
     const size_t o_am = take((size_t)V * Wm * 4);
@@ -798,11 +825,16 @@ struct Runner {
     if (s != GST_OK) return s;
     if (!p) return GST_OK;  // no room: the queries search on their own
     unsigned char* base = (unsigned char*)p;
-    sh.mem = p;
-    sh.bytes = off;
+    // held by the runner from here on (an error below gives it back with the others)
+    shs.emplace_back();
+    shs.back().mem = p;
+    shs.back().bytes = off;
+    shs.back().D = D;
     BsCtx h;
     memset(&h, 0, sizeof(h));
-    h.dist = (uint32_t*)(base + o_dist);
+    h.D = (uint32_t)D;
+    for (int t = 1; t <= D; t++) h.tab[t] = (uint32_t*)(base + o_dist + (size_t)(t - 1) * V * Gp * 4);
+    h.dist = D ? h.tab[D] : (uint32_t*)(base + o_dist);
     h.fm[0] = (uint32_t*)(base + o_fm0);
     h.fm[1] = (uint32_t*)(base + o_fm1);
     h.am = (uint32_t*)(base + o_am);
@@ -811,7 +843,11 @@ struct Runner {
     h.Gp = Gp;
     h.Wm = Wm;
     h.max_steps = (uint32_t)std::min(eng->cfg.max_levels, 1 << 16);
-    h.cut_pm = (uint32_t)(eng->cfg.search_cut_permille > 0 ? eng->cfg.search_cut_permille : 1000);
+    const gst_config& cfg = eng->cfg;
+    h.cut_pm = D ? (cfg.hop_cut_permille > 0
+                        ? (uint32_t)cfg.hop_cut_permille
+                        : 1000u * (uint32_t)(cfg.hop_cut_mult > 0 ? cfg.hop_cut_mult : 1))
+                 : (uint32_t)(cfg.search_cut_permille > 0 ? cfg.search_cut_permille : 1000);
     h.nq = (uint32_t)jobs.size();
     for (size_t q = 0; q < jobs.size(); q++) {
       h.qk[q] = (uint32_t)jobs[q]->q.k;
@@ -829,7 +865,8 @@ struct Runner {
       CK(cudaEventCreate(&eng->bs_ev[1]));
     }
     CK(cudaEventRecord(eng->bs_ev[0], st));
-    CK(cudaMemsetAsync(h.dist, 0xFF, (size_t)V * Gp * 4, st));
+    // the seeds' table (table 1 of a hop-bounded search); the copies fill the others
+    CK(cudaMemsetAsync(D ? h.tab[1] : h.dist, 0xFF, (size_t)V * Gp * 4, st));
     CK(cudaMemsetAsync(h.fm[0], 0, (size_t)V * Wm * 4, st));
     CK(cudaMemsetAsync(h.fm[1], 0, (size_t)V * Wm * 4, st));
     CK(cudaMemcpyAsync(d_b, &h, sizeof(BsCtx), cudaMemcpyHostToDevice, st));
@@ -838,12 +875,17 @@ struct Runner {
     const DevGraph G = dev_graph(g);
     k_bs_seed<<<dim3(16, ncols), 256, 0, st>>>(d_b, G, grp->d_ptr, grp->d_mem, d_cols, (int)ncols);
     int64_t launches = 1;
+    const int64_t n4 = V * (int64_t)Gp / 4;
     int occ = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_bs_relax, 256, 0);
     const int relax_blocks = eng->sms * std::max(1, std::min(occ, 4));
     BsCtx hb;
     for (;;) {
       for (int i = 0; i < 6; i++) {
+        if (D) {
+          k_bs_copy<<<eng->sms * 4, 256, 0, st>>>(d_b, n4, 0);
+          launches++;
+        }
         k_bs_scan<<<eng->sms * 4, 256, 0, st>>>(d_b, G);
         k_bs_relax<<<relax_blocks, 256, 0, st>>>(d_b, G);
         k_bs_ctrl<<<1, 256, 0, st>>>(d_b);
@@ -855,6 +897,11 @@ struct Runner {
       CK(cudaStreamSynchronize(st));
       if (hb.done) break;
     }
+    if (D && hb.round + 1u < (uint32_t)D) {
+      k_bs_copy<<<eng->sms * 4, 256, 0, st>>>(d_b, n4, 1);
+      launches++;
+      CK(cudaGetLastError());
+    }
     CK(cudaEventRecord(eng->bs_ev[1], st));
     CK(cudaEventSynchronize(eng->bs_ev[1]));
     float ms = 0;
@@ -863,11 +910,16 @@ struct Runner {
     cs.bs_sectors += (int64_t)hb.st_relax;
     cs.bs_launches += launches;
     cs.launches += launches;
-    sh.d_b = d_b;
+    Shared& S = shs.back();
     if (hb.error) {  // the queries search on their own
-      shared_release();
+      S.remaining = 0;
+      shared_release(false);
       return GST_OK;
     }
+    S.d_b = d_b;
+    S.Gp = Gp;
+    S.dist = h.dist;
+    for (int t = 0; t <= KMAX; t++) S.tab[t] = h.tab[t];
     // a query's cutoff: the smallest final cutoff of its columns
     for (size_t q = 0; q < jobs.size(); q++) {
       uint32_t cut = COST_INF;
@@ -876,7 +928,7 @@ struct Runner {
       jobs[q]->ss_cut = cut;
       jobs[q]->ss = 1;
     }
-    sh.remaining = (int)jobs.size();
+    S.remaining = (int)jobs.size();
     return GST_OK;
   }
 
@@ -1599,25 +1651,27 @@ namespace {
 // would change it), refilling slots as queries finish; capacity overflows are re-run
 // with more room.  A job that does not fit the free memory yet does not hold back the
 // smaller ones behind it (a batch has no arrival order to keep).
-// A query the batch-shared search may serve: unbounded, a first attempt, not a cache
-// fill, none of its groups in the group cache (those start from exact distances).
-bool shared_eligible(const Runner& R, const Job* j) {
-  if (j->q.hop_bound >= 0 || j->cache_dst || j->boost > 0 || j->ss) return false;
-  for (int i = 0; i < j->q.k; i++)
-    if (R.grp->cache.vec(j->gids[i])) return false;
-  return true;
+// A query the batch-shared search may serve: unbounded or of hop bound 1..KMAX, a first
+// attempt, not a cache fill, none of its groups in the group cache of its kind (those
+// start from exact distances).  Returns its kind (0 unbounded, else D), -1 if none.
+int shared_kind(const Runner& R, const Job* j) {
+  if (j->cache_dst || j->boost > 0 || j->ss) return -1;
+  const int D = j->q.hop_bound;
+  if (D == 0 || D > KMAX) return -1;
+  const auto& hc = R.grp->hop_cache;
+  for (int i = 0; i < j->q.k; i++) {
+    if (D < 0 && R.grp->cache.vec(j->gids[i])) return -1;
+    if (D > 0 && hc.cap > 0 && hc.D == D && hc.vec(j->gids[i])) return -1;
+  }
+  return D < 0 ? 0 : D;
 }
 
-// Before admitting: when no shared table is pending and at least two eligible queries
-// wait, search their groups together (the first eligible queries in order, up to
-// BS_COLS distinct groups and BS_MAXQ queries).
-gst_status maybe_shared_search(Runner& R, std::deque<Job*>& pending) {
-  if (!R.eng->cfg.batch_search || R.sh.remaining > 0) return GST_OK;
-  if (R.sh.mem) R.shared_release();
+// One shared search over the first waiting queries of one kind (0 unbounded, else D).
+gst_status shared_search_kind(Runner& R, std::deque<Job*>& pending, int kind) {
   std::vector<Job*> chunk;
   std::vector<int32_t> cols;
   for (Job* j : pending) {
-    if (!shared_eligible(R, j)) continue;
+    if (shared_kind(R, j) != kind) continue;
     int add = 0;
     for (int i = 0; i < j->q.k; i++)
       add += std::find(cols.begin(), cols.end(), j->gids[i]) == cols.end();
@@ -1627,7 +1681,27 @@ gst_status maybe_shared_search(Runner& R, std::deque<Job*>& pending) {
     chunk.push_back(j);
   }
   if (chunk.size() < 2) return GST_OK;
-  return R.shared_search(chunk, cols);
+  return R.shared_search(chunk, cols, kind);
+}
+
+// Before admitting: for every kind (unbounded, or one hop bound D) with no shared table
+// pending and at least two eligible queries waiting, search their groups together (the
+// first queries of that kind in order, up to BS_COLS distinct groups and BS_MAXQ
+// queries).  Kinds are searched in the order their first queries wait.
+gst_status maybe_shared_search(Runner& R, std::deque<Job*>& pending) {
+  if (!R.eng->cfg.batch_search) return GST_OK;
+  R.shared_release(false);
+  std::vector<int> kinds;
+  for (Job* j : pending) {
+    const int jk = shared_kind(R, j);
+    if (jk >= 0 && !R.shared_of(jk) && std::find(kinds.begin(), kinds.end(), jk) == kinds.end())
+      kinds.push_back(jk);
+  }
+  for (int kind : kinds) {
+    gst_status s = shared_search_kind(R, pending, kind);
+    if (s != GST_OK) return s;
+  }
+  return GST_OK;
 }
 
 gst_status drive(Runner& R, std::deque<Job*>& pending, int B) {
@@ -1647,7 +1721,10 @@ gst_status drive(Runner& R, std::deque<Job*>& pending, int B) {
       }
       if (s == GST_OOM_ADMISSION) {
         Job* j = *it;
-        if (j->ss == 1) R.sh.remaining--;  // never gathers its columns
+        if (j->ss == 1) {  // never gathers its columns
+          Runner::Shared* S = R.shared_of(j->q.hop_bound < 0 ? 0 : j->q.hop_bound);
+          if (S) S->remaining--;
+        }
         j->out->status = GST_OOM_ADMISSION;
         j->out->user_tag = j->q.user_tag;
         fail(eng, GST_OOM_ADMISSION, "solve: the query's state table does not fit the memory budget");
@@ -1657,6 +1734,14 @@ gst_status drive(Runner& R, std::deque<Job*>& pending, int B) {
       }
       it = pending.erase(it);
     }
+    if (st == GST_OK && R.active == 0 && !pending.empty() && !R.shs.empty()) {
+      // nothing runs and the shared tables hold memory a waiting query needs: give them
+      // back; the waiting queries search on their own
+      for (Job* j : pending)
+        if (j->ss == 1) j->ss = 2;
+      R.shared_release(true);
+      continue;
+    }
     if (st != GST_OK || R.active == 0) break;
     st = R.run(0);
     done.clear();
@@ -1664,7 +1749,7 @@ gst_status drive(Runner& R, std::deque<Job*>& pending, int B) {
     if (st == GST_OK) st = R.harvest(done, retry);
     for (Job* j : retry) pending.push_front(j);
   }
-  R.shared_release();
+  R.shared_release(true);
   R.max_slots = saved;
   return st;
 }

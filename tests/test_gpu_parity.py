@@ -280,18 +280,19 @@ def test_search_cutoff_keeps_optima(permille):
 
 
 def test_shared_search_matches_alone(engine):
-    """The unbounded queries of a batch search their groups' distances together (one
-    table of up to 256 groups, at most 64 queries per search, here two searches): every
-    optimum equals the query solved alone and the oracle's, and the trees verify.
-    Hop-bounded queries in the same batch keep their own searches."""
+    """The queries of a batch search their groups' distances together, one search per
+    kind (unbounded, or one hop bound D: D tables of paths of at most 1..D edges), at most
+    256 groups and 64 queries per search: every optimum equals the query solved alone and
+    the oracle's, and the trees verify."""
     rng = np.random.default_rng(61)
     g = G.synth_rmat(3000, 14000, 62)
     grp = G.synth_groups_zipf(g.V, 400, 1.5, 1, 60, 63)
+    kinds = [None, None, None, 3, 2, 4, 1]
     qs, hops = [], []
-    for t in range(80):
+    for t in range(100):
         k = int(rng.integers(2, 7))
         qs.append(rng.choice(grp.n_groups, size=k, replace=False).astype(np.int32))
-        hops.append(3 if t % 9 == 4 else None)
+        hops.append(kinds[t % len(kinds)])
     dg = engine.graph(g, grp)
     try:
         alone = [dg.solve(q, h) for q, h in zip(qs, hops)]
@@ -301,8 +302,14 @@ def test_shared_search_matches_alone(engine):
             assert a.status == b.status and (not a.ok or a.cost == b.cost), (q, h, a.cost, b.cost)
             if b.ok:
                 assert G.verify_tree(g, grp, q, -1 if h is None else h, b.cost, b.edges, b.root) == 0
-        for q, h, b in list(zip(qs, hops, mixed))[:8]:
+        for q, h, b in list(zip(qs, hops, mixed))[:14]:
             o = O.gst_nonhop(g, grp, q) if h is None else O.gst_hop(g, grp, q, h)
             assert (b.cost if b.ok else -1) == o["cost"], (q, h)
+        # a batch of one hop bound alone: its search is shared
+        hq = [q for q, h in zip(qs, hops) if h == 3]
+        hb = dg.solve_batch(hq, [3] * len(hq))
+        assert hb[0].stats["shared_launches"] > 0
+        for q, a, b in zip(hq, [a for a, h in zip(alone, hops) if h == 3], hb):
+            assert a.status == b.status and (not a.ok or a.cost == b.cost), (q, a.cost, b.cost)
     finally:
         dg.close()
