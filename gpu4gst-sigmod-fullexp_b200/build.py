@@ -24,7 +24,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CU_SOURCES = ["gst_engine.cu", "gst_probe.cu"]
 CPP_SOURCES = ["gst_io.cpp", "gst_synth.cpp"]
-HEADERS = ["gst_device.cuh"]
+# every device header of csrc/ (a kernel edited in any of them rebuilds its sources)
+HEADERS = sorted(f for f in os.listdir(os.path.join(HERE, "csrc")) if f.endswith((".cuh", ".h")))
 LIB = os.path.join(HERE, "libgst_b200.so")
 CLI = {"gst_nonhop": "gst_cli.cpp", "gst_hop": "gst_cli.cpp"}
 

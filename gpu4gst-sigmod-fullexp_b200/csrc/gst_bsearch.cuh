@@ -128,23 +128,30 @@ __global__ void k_bs_scan(BsCtx* b, DevGraph G) {
   }
 }
 
-// Relax: one item per warp iteration.  Lane s holds columns 8s..8s+7 of the item's
-// vertex (its distances, cutoffs and active bits); for each edge of the item's chunk the
-// lanes with active columns read their sector of the target's row, relax, and announce
-// the improved columns.  The first chunk of a vertex also sums each query's columns
-// there (a star: the query's k shortest paths from v form a connected subgraph covering
-// every group, a feasible cost).
+// Relax: one item per warp iteration, in two phases.  First lane s holds sector s
+// (columns 8s..8s+7) of the item's vertex: its distances, active bits and, per active
+// column, the heaviest edge it may still take (`lim`); the first chunk of a vertex also
+// sums each query's columns there (a star: the query's k shortest paths from v form a
+// connected subgraph covering every group, a feasible cost).  Then the work is the
+// item's edges times its nA sectors with an active column, spread over all 32 lanes:
+// lane t takes active sector t mod nA and the edges t / nA, t / nA + R, ... (R = 32 /
+// nA), reading that sector of each target's row, relaxing and announcing the improved
+// columns.  The kernel is bound by instruction issue, not memory (a row is one
+// contiguous span), and an item rarely has more than a few active sectors, so the
+// edge loop is what the compaction keeps busy.
 __global__ void __launch_bounds__(256, 4) k_bs_relax(BsCtx* b, DevGraph G) {
   __shared__ uint32_t s_cut[BS_COLS];
   __shared__ uint32_t s_row[256 / 32][BS_COLS];  // per warp: the first chunk's full row
+  __shared__ uint16_t s_split[33][32];           // [nA][t]: t mod nA | (t / nA) << 8
+  __shared__ unsigned char s_map[256 / 32][32];  // per warp: active index -> sector
   if (b->done) return;
   const uint32_t Gp = b->Gp, Wm = b->Wm, nsec = Gp / 8u, nq = b->nq;
   for (uint32_t c = threadIdx.x; c < BS_COLS; c += blockDim.x) s_cut[c] = c < Gp ? b->cutc[c] : 0u;
+  for (uint32_t x = threadIdx.x; x < 33u * 32u; x += blockDim.x) {
+    const uint32_t na = x >> 5, t = x & 31u;
+    s_split[na][t] = na ? (uint16_t)((t % na) | ((t / na) << 8)) : 0;
+  }
   __syncthreads();
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const uint32_t n = min(b->n_items, b->item_cap);
-  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-  uint32_t* fo = b->fm[b->in ^ 1u];
   // hop-bounded round r: sources in table r (the members at 0 for r = 0), targets in
   // table r + 1; a round's paths extend only while they have fewer than D edges; stars
   // from tables r with 2r <= D
@@ -154,28 +161,30 @@ __global__ void __launch_bounds__(256, 4) k_bs_relax(BsCtx* b, DevGraph G) {
   uint32_t* dst_tab = D ? b->tab[r + 1] : b->dist;
   const bool extend = D == 0u || r + 1u < D;
   const bool stars = D == 0u || (r >= 1u && 2u * r <= D);
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const uint32_t n = min(b->n_items, b->item_cap);
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  uint32_t* fo = b->fm[b->in ^ 1u];
+  const bool mine = (uint32_t)lane < nsec;
+  const uint32_t s = (uint32_t)lane;
   // per lane: best star of queries lane and lane + 32 over the warp's items
   uint32_t star0 = COST_INF, star1 = COST_INF;
   unsigned long long relaxed = 0;
   uint32_t any = 0;
-  const bool mine = (uint32_t)lane < nsec;
-  const uint32_t s = (uint32_t)lane;
   for (uint32_t it = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; it < n; it += warps) {
     const uint2 item = b->items[it];
     const uint32_t v = item.x, chunk = item.y;
     uint32_t m = 0;
     if (mine) m = (__ldcg(&b->am[(uint64_t)v * Wm + (s >> 2)]) >> ((s & 3u) * 8u)) & 0xFFu;
-    uint32_t dv[8], cut[8];
+    const bool dostar = chunk == 0 && stars;
+    uint32_t dv[8];
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
-      dv[i] = COST_INF;
-      cut[i] = mine ? s_cut[s * 8 + i] : 0u;
-    }
+    for (int i = 0; i < 8; i++) dv[i] = COST_INF;
     if (mine && !src_tab) {
 #pragma unroll
       for (int i = 0; i < 8; i++)
         if ((m >> i) & 1u) dv[i] = 0u;  // round 0: the members themselves
-    } else if (mine && (m || (chunk == 0 && stars))) {
+    } else if (mine && (m || dostar)) {
       const uint4* src = (const uint4*)&src_tab[(uint64_t)v * Gp + s * 8];
       const uint4 a = __ldcg(src), c4 = __ldcg(src + 1);
       dv[0] = a.x;
@@ -187,7 +196,7 @@ __global__ void __launch_bounds__(256, 4) k_bs_relax(BsCtx* b, DevGraph G) {
       dv[6] = c4.z;
       dv[7] = c4.w;
     }
-    if (chunk == 0 && stars) {
+    if (dostar) {
       // stars of every query at v (v's row in shared memory, one query per lane)
       if (mine) {
 #pragma unroll
@@ -204,48 +213,66 @@ __global__ void __launch_bounds__(256, 4) k_bs_relax(BsCtx* b, DevGraph G) {
       }
       __syncwarp();
     }
-    // the heaviest edge any active column may still take from v
-    uint32_t wl = 0, amask = 0;
+    // per active column: the heaviest edge it may still take from v (0: none; edge
+    // weights are at least 1), and for the warp the heaviest of them all
+    uint32_t lim[8], wl = 0;
 #pragma unroll
-    for (int i = 0; i < 8; i++)
-      if (((m >> i) & 1u) && dv[i] < cut[i]) {
-        wl = max(wl, cut[i] - dv[i]);
-        amask |= 1u << i;
-      }
+    for (int i = 0; i < 8; i++) {
+      const uint32_t cut = mine ? s_cut[s * 8 + i] : 0u;
+      lim[i] = (((m >> i) & 1u) && dv[i] < cut) ? cut - dv[i] : 0u;
+      wl = max(wl, lim[i]);
+    }
+    const uint32_t amask = __ballot_sync(0xffffffffu, wl != 0u);
     wl = __reduce_max_sync(0xffffffffu, wl);
+    if (!amask) continue;
     const int64_t b0 = G.beg[v], b1 = G.beg[v + 1];
     const int64_t cnt = count_upto(G, v, b1 - b0, wl);
     const int64_t e0 = (int64_t)chunk * BS_CHUNK, e1 = min(cnt, e0 + BS_CHUNK);
-    const bool act = amask != 0u;
-    // work: the target-row sectors this item reads, one per active lane and edge
-    const uint32_t nact = (uint32_t)__popc(__ballot_sync(0xffffffffu, act));
-    if (e1 > e0) relaxed += (unsigned long long)(e1 - e0) * nact;
-    int2 ed = e0 < e1 ? G.wedges[b0 + e0] : make_int2(0, 0);
-    for (int64_t e = e0; e < e1; e++) {
+    if (e1 <= e0) continue;
+    // work: the target-row sectors this item reads, one per active sector and edge
+    const uint32_t nA = (uint32_t)__popc(amask);
+    relaxed += (unsigned long long)(e1 - e0) * nA;
+    // compaction: active index -> sector, then each lane takes its sector's values
+    if ((amask >> lane) & 1u) s_map[wib][__popc(amask & ((1u << lane) - 1u))] = (unsigned char)lane;
+    __syncwarp();
+    const uint32_t sp = s_split[nA][lane];
+    const uint32_t R = 32u / nA;  // edges per round (warp-uniform)
+    const uint32_t sec = s_map[wib][sp & 0xFFu];
+    const int64_t joff = (int64_t)(sp >> 8);
+    uint32_t dx[8], lx[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      dx[i] = __shfl_sync(0xffffffffu, dv[i], (int)sec);
+      lx[i] = __shfl_sync(0xffffffffu, lim[i], (int)sec);
+    }
+    if (joff >= (int64_t)R) continue;  // lanes beyond R x nA
+    int64_t e = e0 + joff;
+    int2 ed = e < e1 ? G.wedges[b0 + e] : make_int2(0, 0);
+    for (; e < e1; e += R) {
       const uint32_t u = (uint32_t)ed.x, w = (uint32_t)ed.y;
       uint4 ra = make_uint4(0, 0, 0, 0), rb = ra;
-      const bool go = act && u < G.V;
+      const bool go = u < G.V;
       if (go) {
-        const uint4* dst = (const uint4*)&dst_tab[(uint64_t)u * Gp + s * 8];
+        const uint4* dst = (const uint4*)&dst_tab[(uint64_t)u * Gp + sec * 8];
         ra = __ldcg(dst);
         rb = __ldcg(dst + 1);
       }
-      if (e + 1 < e1) ed = G.wedges[b0 + e + 1];
+      if (e + R < e1) ed = G.wedges[b0 + e + R];
       if (go) {
         const uint32_t du[8] = {ra.x, ra.y, ra.z, ra.w, rb.x, rb.y, rb.z, rb.w};
         uint32_t imp = 0;
 #pragma unroll
         for (int i = 0; i < 8; i++) {
-          if (((amask >> i) & 1u) && w <= cut[i] - dv[i]) {
-            const uint32_t nd = dv[i] + w;
+          if (w <= lx[i]) {
+            const uint32_t nd = dx[i] + w;
             if (nd < du[i]) {
-              atomicMin(&dst_tab[(uint64_t)u * Gp + s * 8 + i], nd);
-              if (nd < cut[i] && extend) imp |= 1u << i;
+              atomicMin(&dst_tab[(uint64_t)u * Gp + sec * 8 + i], nd);
+              if (w < lx[i] && extend) imp |= 1u << i;
             }
           }
         }
         if (imp) {
-          atomicOr(&fo[(uint64_t)u * Wm + (s >> 2)], imp << ((s & 3u) * 8u));
+          atomicOr(&fo[(uint64_t)u * Wm + (sec >> 2)], imp << ((sec & 3u) * 8u));
           any = 1u;
         }
       }

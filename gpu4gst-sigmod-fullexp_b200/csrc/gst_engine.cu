@@ -353,7 +353,7 @@ void init_query_ctx(Ctx& c, const gst_query* q, const gst_config& cfg) {
   c.sssp_mask = c.sssp_hops ? 2u : (c.bucket_end == 0xFFFFFFFFu ? 1u : 0u);
 }
 
-enum ProfKind { PROF_GROW = 0, PROF_ROWS = 1, PROF_SSSP = 2 };
+enum ProfKind { PROF_GROW = 0, PROF_ROWS = 1, PROF_SSSP = 2, PROF_BSRELAX = 3, PROF_KINDS = 4 };
 
 // A query waiting for, or holding, a slot.
 struct Job {
@@ -383,7 +383,7 @@ struct CallStats {
   int64_t graph_launches = 0, graph_levels = 0;
   int64_t allocs = 0, alloc_bytes = 0;
   double alloc_ms = 0;
-  int64_t bs_sectors = 0, bs_launches = 0;  // batch-shared searches of the call
+  int64_t bs_sectors = 0, bs_launches = 0, bs_relax = 0;  // batch-shared searches of the call
   double bs_ms = 0;
   std::vector<std::pair<int, int>> prof;  // (kernel kind, event-pair index)
   size_t next_ev = 0;
@@ -874,7 +874,7 @@ struct Runner {
     cs.h2d += sizeof(BsCtx) + ncols * 4;
     const DevGraph G = dev_graph(g);
     k_bs_seed<<<dim3(16, ncols), 256, 0, st>>>(d_b, G, grp->d_ptr, grp->d_mem, d_cols, (int)ncols);
-    int64_t launches = 1;
+    int64_t launches = 1, relax_launches = 0;
     const int64_t n4 = V * (int64_t)Gp / 4;
     int occ = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_bs_relax, 256, 0);
@@ -887,7 +887,10 @@ struct Runner {
           launches++;
         }
         k_bs_scan<<<eng->sms * 4, 256, 0, st>>>(d_b, G);
+        const int pe = prof_begin(PROF_BSRELAX);
         k_bs_relax<<<relax_blocks, 256, 0, st>>>(d_b, G);
+        prof_end(pe);
+        relax_launches++;
         k_bs_ctrl<<<1, 256, 0, st>>>(d_b);
         launches += 3;
       }
@@ -909,6 +912,7 @@ struct Runner {
     cs.bs_ms += ms;
     cs.bs_sectors += (int64_t)hb.st_relax;
     cs.bs_launches += launches;
+    cs.bs_relax += relax_launches;
     cs.launches += launches;
     Shared& S = shs.back();
     if (hb.error) {  // the queries search on their own
@@ -1217,10 +1221,12 @@ struct Runner {
     }
   }
 
-  // Summed profiled kernel time of this call (grow, rows, sssp), in ms, and launches.
-  void kernel_ms(double out[3], int64_t n[3]) {
-    out[0] = out[1] = out[2] = 0;
-    n[0] = n[1] = n[2] = 0;
+  // Summed profiled kernel time of this call per ProfKind, in ms, and launches.
+  void kernel_ms(double out[PROF_KINDS], int64_t n[PROF_KINDS]) {
+    for (int i = 0; i < PROF_KINDS; i++) {
+      out[i] = 0;
+      n[i] = 0;
+    }
     for (auto& pr : cs.prof) {
       float e = 0;
       if (cudaEventElapsedTime(&e, eng->prof_events[2 * pr.second],
@@ -1452,7 +1458,7 @@ gst_status gst_engine_destroy(gst_engine* eng) {
 }
 
 gst_status gst_engine_set_profiling(gst_engine* eng, int32_t bits) {
-  if (!eng || bits < 0 || bits > 7) return fail(eng, GST_BAD_INPUT, "profiling: bits must be in [0, 7]");
+  if (!eng || bits < 0 || bits > 15) return fail(eng, GST_BAD_INPUT, "profiling: bits must be in [0, 15]");
   std::lock_guard<std::mutex> lk(eng->mu);
   eng->cfg.profile_kernels = bits;
   return GST_OK;
@@ -1941,8 +1947,8 @@ gst_status gst_solve_batch(gst_graph* g, gst_groups* grp, int32_t n, const gst_q
             "%lld slot allocations (%.1f GB, %.1f ms host)\n",
             n, ms, (long long)R.cs.launches, (long long)R.cs.graph_launches,
             (long long)R.cs.graph_levels, (long long)R.cs.allocs, R.cs.alloc_bytes / 1e9, R.cs.alloc_ms);
-  double kms[3];
-  int64_t kn[3];
+  double kms[PROF_KINDS];
+  int64_t kn[PROF_KINDS];
   R.kernel_ms(kms, kn);
   for (int32_t i = 0; i < n; i++) {
     gst_stats& s = results[i].stats;
@@ -1956,9 +1962,11 @@ gst_status gst_solve_batch(gst_graph* g, gst_groups* grp, int32_t n, const gst_q
     s.grow_launches = kn[PROF_GROW];
     s.rows_launches = kn[PROF_ROWS];
     s.sssp_launches = kn[PROF_SSSP];
+    s.shared_relax_ms = kms[PROF_BSRELAX];
     s.shared_sectors = R.cs.bs_sectors;
     s.shared_ms = R.cs.bs_ms;
     s.shared_launches = R.cs.bs_launches;
+    s.shared_relax_launches = R.cs.bs_relax;
   }
   return GST_OK;
 }

@@ -292,7 +292,8 @@ class Stats(C.Structure):
                 ("queue_max", C.c_int64), ("grow_launches", C.c_int64),
                 ("rows_launches", C.c_int64), ("sssp_launches", C.c_int64),
                 ("shared_sectors", C.c_int64), ("shared_ms", C.c_double),
-                ("shared_launches", C.c_int64)]
+                ("shared_launches", C.c_int64), ("shared_relax_launches", C.c_int64),
+                ("shared_relax_ms", C.c_double)]
 
 
 class Result(C.Structure):

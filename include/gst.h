@@ -68,8 +68,9 @@ typedef struct gst_config {
   int32_t use_graphs;         /* 1 (default): run the level loop as a CUDA graph whose
                                  conditional WHILE node repeats the level body on the device
                                  until a query finishes; ignored while profile_kernels != 0 */
-  int32_t profile_kernels;    /* bit0 grow, bit1 rows, bit2 sssp: bracket those launches with
-                                 CUDA events and report their summed device time */
+  int32_t profile_kernels;    /* bit0 grow, bit1 rows, bit2 sssp, bit3 the shared search's relax
+                                 steps: bracket those launches with CUDA events and report
+                                 their summed device time */
   int32_t verbose;
   int32_t hop_cut_mult;       /* hop-bounded queries: the distance search stops at this
                                  multiple of the star bound (0 = 1); larger prunes more
@@ -115,7 +116,9 @@ typedef struct gst_stats {
   int64_t shared_sectors;   /* batch-shared distance search of the call: target-row sectors
                                read (edges x active 8-group sectors), */
   double shared_ms;         /*   its device time, */
-  int64_t shared_launches;  /*   and its kernel launches */
+  int64_t shared_launches;  /*   and its kernel launches, */
+  int64_t shared_relax_launches; /* of which relax steps (k_bs_relax), */
+  double shared_relax_ms;   /*   their device time (0 unless profile_kernels bit3) */
 } gst_stats;
 
 typedef struct gst_result {
@@ -132,9 +135,9 @@ typedef struct gst_result {
 } gst_result;
 
 void gst_config_default(gst_config* cfg);
-/* Change cfg.profile_kernels of a live engine (bit0 grow, bit1 rows, bit2 sssp); the
- * next solve brackets those launches with CUDA events (and runs the level loop
- * without the CUDA graph while any bit is set). */
+/* Change cfg.profile_kernels of a live engine (bit0 grow, bit1 rows, bit2 sssp, bit3 the
+ * shared search's relax steps); the next solve brackets those launches with CUDA events
+ * (and runs the level loop without the CUDA graph while any bit is set). */
 gst_status gst_engine_set_profiling(gst_engine* eng, int32_t bits);
 
 gst_status gst_engine_create(int32_t device, const gst_config* cfg, gst_engine** out);
