@@ -144,9 +144,11 @@ __global__ void __launch_bounds__(256, 4) k_bs_relax(BsCtx* b, DevGraph G) {
   __shared__ uint32_t s_row[256 / 32][BS_COLS];  // per warp: the first chunk's full row
   __shared__ uint16_t s_split[33][32];           // [nA][t]: t mod nA | (t / nA) << 8
   __shared__ unsigned char s_map[256 / 32][32];  // per warp: active index -> sector
+  __shared__ uint32_t s_star[BS_MAXQ];           // the block's best star per query
   if (b->done) return;
   const uint32_t Gp = b->Gp, Wm = b->Wm, nsec = Gp / 8u, nq = b->nq;
   for (uint32_t c = threadIdx.x; c < BS_COLS; c += blockDim.x) s_cut[c] = c < Gp ? b->cutc[c] : 0u;
+  for (uint32_t q = threadIdx.x; q < BS_MAXQ; q += blockDim.x) s_star[q] = COST_INF;
   for (uint32_t x = threadIdx.x; x < 33u * 32u; x += blockDim.x) {
     const uint32_t na = x >> 5, t = x & 31u;
     s_split[na][t] = na ? (uint16_t)((t % na) | ((t / na) << 8)) : 0;
@@ -167,8 +169,6 @@ __global__ void __launch_bounds__(256, 4) k_bs_relax(BsCtx* b, DevGraph G) {
   uint32_t* fo = b->fm[b->in ^ 1u];
   const bool mine = (uint32_t)lane < nsec;
   const uint32_t s = (uint32_t)lane;
-  // per lane: best star of queries lane and lane + 32 over the warp's items
-  uint32_t star0 = COST_INF, star1 = COST_INF;
   unsigned long long relaxed = 0;
   uint32_t any = 0;
   for (uint32_t it = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; it < n; it += warps) {
@@ -206,10 +206,7 @@ __global__ void __launch_bounds__(256, 4) k_bs_relax(BsCtx* b, DevGraph G) {
       for (uint32_t q = (uint32_t)lane; q < nq; q += 32) {
         uint64_t sum = 0;
         for (uint32_t i = 0; i < b->qk[q]; i++) sum += s_row[wib][b->qcol[q][i]];
-        if (sum < COST_INF) {
-          if (q < 32) star0 = min(star0, (uint32_t)sum);
-          else star1 = min(star1, (uint32_t)sum);
-        }
+        if (sum < (uint64_t)s_star[q]) atomicMin(&s_star[q], (uint32_t)sum);
       }
       __syncwarp();
     }
@@ -247,19 +244,40 @@ __global__ void __launch_bounds__(256, 4) k_bs_relax(BsCtx* b, DevGraph G) {
     }
     if (joff >= (int64_t)R) continue;  // lanes beyond R x nA
     int64_t e = e0 + joff;
-    int2 ed = e < e1 ? G.wedges[b0 + e] : make_int2(0, 0);
-    for (; e < e1; e += R) {
-      const uint32_t u = (uint32_t)ed.x, w = (uint32_t)ed.y;
-      uint4 ra = make_uint4(0, 0, 0, 0), rb = ra;
-      const bool go = u < G.V;
-      if (go) {
-        const uint4* dst = (const uint4*)&dst_tab[(uint64_t)u * Gp + sec * 8];
-        ra = __ldcg(dst);
-        rb = __ldcg(dst + 1);
+    // the edges are sorted by weight: a lane stops at the first one heavier than every
+    // limit of its sector; two edges per lane in flight
+    uint32_t lmax = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) lmax = max(lmax, lx[i]);
+    const int64_t R2 = 2 * (int64_t)R;
+    int2 ea = e < e1 ? G.wedges[b0 + e] : make_int2(0, 0);
+    int2 eb = e + R < e1 ? G.wedges[b0 + e + R] : make_int2(0, 0);
+    for (; e < e1; e += R2) {
+      const bool hb = e + R < e1;
+      const uint32_t ua = (uint32_t)ea.x, wa = (uint32_t)ea.y;
+      const uint32_t ub = (uint32_t)eb.x, wb = (uint32_t)eb.y;
+      if (wa > lmax) break;
+      const bool ga = ua < G.V, gb = hb && wb <= lmax && ub < G.V;
+      uint4 ra0 = make_uint4(0, 0, 0, 0), ra1 = ra0, rb0 = ra0, rb1 = ra0;
+      if (ga) {
+        const uint4* dst = (const uint4*)&dst_tab[(uint64_t)ua * Gp + sec * 8];
+        ra0 = __ldcg(dst);
+        ra1 = __ldcg(dst + 1);
       }
-      if (e + R < e1) ed = G.wedges[b0 + e + R];
-      if (go) {
-        const uint32_t du[8] = {ra.x, ra.y, ra.z, ra.w, rb.x, rb.y, rb.z, rb.w};
+      if (gb) {
+        const uint4* dst = (const uint4*)&dst_tab[(uint64_t)ub * Gp + sec * 8];
+        rb0 = __ldcg(dst);
+        rb1 = __ldcg(dst + 1);
+      }
+      if (e + R2 < e1) ea = G.wedges[b0 + e + R2];
+      if (e + R2 + R < e1) eb = G.wedges[b0 + e + R2 + R];
+#pragma unroll
+      for (int x = 0; x < 2; x++) {
+        const bool g = x ? gb : ga;
+        const uint32_t u = x ? ub : ua, w = x ? wb : wa;
+        const uint4 r0 = x ? rb0 : ra0, r1 = x ? rb1 : ra1;
+        if (!g) continue;
+        const uint32_t du[8] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
         uint32_t imp = 0;
 #pragma unroll
         for (int i = 0; i < 8; i++) {
@@ -280,9 +298,10 @@ __global__ void __launch_bounds__(256, 4) k_bs_relax(BsCtx* b, DevGraph G) {
   }
   any = __reduce_or_sync(0xffffffffu, any);
   if (lane == 0 && any) b->ann = 1u;
-  if (star0 < COST_INF && lane < (int)nq) atomicMin(&b->star[lane], star0);
-  if (star1 < COST_INF && lane + 32 < (int)nq) atomicMin(&b->star[lane + 32], star1);
   if (lane == 0 && relaxed) atomicAdd(&b->st_relax, relaxed);  // the same in every lane
+  __syncthreads();
+  for (uint32_t q = threadIdx.x; q < nq; q += blockDim.x)
+    if (s_star[q] < COST_INF) atomicMin(&b->star[q], s_star[q]);
 }
 
 // Hop-bounded tables (n4 = V x Gp / 4 uint4 per table).  Before round r >= 1:

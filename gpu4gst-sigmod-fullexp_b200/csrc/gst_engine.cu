@@ -1271,6 +1271,13 @@ struct gst_server {
   int64_t admitted = 0, completed = 0;
 };
 
+// defined with the batch driver below (inside its extern "C" block)
+extern "C" {
+namespace {
+gst_status maybe_shared_search(Runner& R, std::deque<Job*>& pending);
+}  // namespace
+}  // extern "C"
+
 namespace {
 
 void server_loop(gst_server* sv) {
@@ -1294,7 +1301,18 @@ void server_loop(gst_server* sv) {
     {
       std::lock_guard<std::mutex> elk(eng->mu);
       cudaSetDevice(eng->device);
+      // the waiting arrivals' distances: one shared search per kind, as in a batch call
+      gst_status s_pre = GST_OK;
+      if (eng->cfg.batch_search) {
+        std::deque<Job*> snap;
+        {
+          std::lock_guard<std::mutex> lk(sv->mu);
+          snap = sv->pending;
+        }
+        s_pre = maybe_shared_search(R, snap);
+      }
       for (;;) {
+        if (s_pre != GST_OK) break;
         Job* j = nullptr;
         {
           std::lock_guard<std::mutex> lk(sv->mu);
@@ -1321,13 +1339,21 @@ void server_loop(gst_server* sv) {
         std::lock_guard<std::mutex> lk(sv->mu);
         waiting = !sv->pending.empty();
       }
-      gst_status s = GST_OK;
+      gst_status s = s_pre;
+      if (s == GST_OK && R.active == 0 && waiting && !R.shs.empty()) {
+        // nothing runs and the shared tables hold memory the next arrival needs: give
+        // them back; the waiting queries search on their own
+        std::lock_guard<std::mutex> lk(sv->mu);
+        for (Job* j : sv->pending)
+          if (j->ss == 1) j->ss = 2;
+        R.shared_release(true);
+      }
       if (eng->cfg.verbose) {
         std::lock_guard<std::mutex> lk(sv->mu);
         fprintf(stderr, "[gst server] active %d pending %zu held %zu budget %zu\n", R.active,
                 sv->pending.size(), R.held, R.budget);
       }
-      if (R.active > 0) {
+      if (s == GST_OK && R.active > 0) {
         // with arrivals waiting for a slot, come back at the next finished query;
         // with free slots and arrivals possible, check every few levels
         const bool free_slot = R.active < R.max_slots;
@@ -1658,17 +1684,20 @@ namespace {
 // with more room.  A job that does not fit the free memory yet does not hold back the
 // smaller ones behind it (a batch has no arrival order to keep).
 // A query the batch-shared search may serve: unbounded or of hop bound 1..KMAX, a first
-// attempt, not a cache fill, none of its groups in the group cache of its kind (those
-// start from exact distances).  Returns its kind (0 unbounded, else D), -1 if none.
+// attempt, not a cache fill, not every group in the group cache of its kind (those start
+// from exact distances; with only some cached, the shared table serves all of them).
+// Returns its kind (0 unbounded, else D), -1 if none.
 int shared_kind(const Runner& R, const Job* j) {
   if (j->cache_dst || j->boost > 0 || j->ss) return -1;
   const int D = j->q.hop_bound;
   if (D == 0 || D > KMAX) return -1;
   const auto& hc = R.grp->hop_cache;
+  int cached = 0;
   for (int i = 0; i < j->q.k; i++) {
-    if (D < 0 && R.grp->cache.vec(j->gids[i])) return -1;
-    if (D > 0 && hc.cap > 0 && hc.D == D && hc.vec(j->gids[i])) return -1;
+    if (D < 0) cached += R.grp->cache.vec(j->gids[i]) != nullptr;
+    if (D > 0) cached += hc.cap > 0 && hc.D == D && hc.vec(j->gids[i]) != nullptr;
   }
+  if (cached == j->q.k) return -1;
   return D < 0 ? 0 : D;
 }
 
