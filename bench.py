@@ -860,7 +860,7 @@ def run_profile_batch(args):
     summaries in profiles/ give the commands)."""
     import gst_b200 as G
     w, g, grp, queries, hops = make_workload(args.workload)
-    eng = G.Engine(0, max_batch=args.batch, use_graphs=0)
+    eng = G.Engine(0, max_batch=args.resident or args.batch, use_graphs=0)
     dg = eng.graph(g, grp)
     qs, hs = queries[: args.batch], hops[: args.batch]
     dg.solve_batch(qs, hs)
@@ -909,6 +909,8 @@ def main():
     ap.add_argument("--profile-batch", action="store_true",
                     help="one batch of the first --batch queries with per-kernel launches "
                          "after one untimed batch; prints algorithmic bytes per kernel")
+    ap.add_argument("--resident", type=int, default=0,
+                    help="with --profile-batch: queries resident at once (default: the batch)")
     args = ap.parse_args()
     if args.profile_batch:
         return run_profile_batch(args)

@@ -12,8 +12,8 @@
 //
 // Cutoffs: a query's distances are needed exactly only up to its search cutoff (its star
 // bound x cut_pm / 1000).  Column c keeps the largest cutoff of the queries that use it;
-// stars are found while the search runs (the relax kernel, for each announced vertex,
-// sums each query's columns there) and the cutoffs only decrease, so every distance at
+// stars are found while the search runs (before each relax step, k_bs_star sums each
+// query's columns at every announced vertex) and the cutoffs only decrease, so every distance at
 // most a column's final cutoff is exact (every prefix of its shortest path stayed below
 // it) and every other one is only known to exceed it.  A query then takes the smallest
 // final cutoff of its columns as its own `cut` (distances above it are clamped to cut + 1
@@ -31,8 +31,10 @@
 // it are filled from it.
 //
 // Per step: k_bs_scan turns the announcement bits of the previous step into relax items
-// of at most BS_CHUNK edges (a hub's range spread over many warps), k_bs_relax relaxes
-// them, k_bs_ctrl updates the cutoffs and ends the search when nothing was announced.
+// of at most BS_CHUNK edges (a hub's range spread over many warps), k_bs_star finds the
+// stars at the announced vertices and k_bs_ctrl lowers the cutoffs, k_bs_relax relaxes
+// the items, and k_bs_ctrl updates the cutoffs again and ends the search when nothing
+// was announced.
 #pragma once
 #include "gst_device.cuh"
 
@@ -130,9 +132,7 @@ __global__ void k_bs_scan(BsCtx* b, DevGraph G) {
 
 // Relax: one item per warp iteration, in two phases.  First lane s holds sector s
 // (columns 8s..8s+7) of the item's vertex: its distances, active bits and, per active
-// column, the heaviest edge it may still take (`lim`); the first chunk of a vertex also
-// sums each query's columns there (a star: the query's k shortest paths from v form a
-// connected subgraph covering every group, a feasible cost).  Then the work is the
+// column, the heaviest edge it may still take (`lim`).  Then the work is the
 // item's edges times its nA sectors with an active column, spread over all 32 lanes:
 // lane t takes active sector t mod nA and the edges t / nA, t / nA + R, ... (R = 32 /
 // nA), reading that sector of each target's row, relaxing and announcing the improved
@@ -141,28 +141,23 @@ __global__ void k_bs_scan(BsCtx* b, DevGraph G) {
 // edge loop is what the compaction keeps busy.
 __global__ void __launch_bounds__(256, 4) k_bs_relax(BsCtx* b, DevGraph G) {
   __shared__ uint32_t s_cut[BS_COLS];
-  __shared__ uint32_t s_row[256 / 32][BS_COLS];  // per warp: the first chunk's full row
   __shared__ uint16_t s_split[33][32];           // [nA][t]: t mod nA | (t / nA) << 8
   __shared__ unsigned char s_map[256 / 32][32];  // per warp: active index -> sector
-  __shared__ uint32_t s_star[BS_MAXQ];           // the block's best star per query
   if (b->done) return;
-  const uint32_t Gp = b->Gp, Wm = b->Wm, nsec = Gp / 8u, nq = b->nq;
+  const uint32_t Gp = b->Gp, Wm = b->Wm, nsec = Gp / 8u;
   for (uint32_t c = threadIdx.x; c < BS_COLS; c += blockDim.x) s_cut[c] = c < Gp ? b->cutc[c] : 0u;
-  for (uint32_t q = threadIdx.x; q < BS_MAXQ; q += blockDim.x) s_star[q] = COST_INF;
   for (uint32_t x = threadIdx.x; x < 33u * 32u; x += blockDim.x) {
     const uint32_t na = x >> 5, t = x & 31u;
     s_split[na][t] = na ? (uint16_t)((t % na) | ((t / na) << 8)) : 0;
   }
   __syncthreads();
   // hop-bounded round r: sources in table r (the members at 0 for r = 0), targets in
-  // table r + 1; a round's paths extend only while they have fewer than D edges; stars
-  // from tables r with 2r <= D
+  // table r + 1; a round's paths extend only while they have fewer than D edges
   const uint32_t D = b->D, r = b->round;
   if (D && r >= D) return;
   const uint32_t* src_tab = D ? (r ? b->tab[r] : nullptr) : b->dist;
   uint32_t* dst_tab = D ? b->tab[r + 1] : b->dist;
   const bool extend = D == 0u || r + 1u < D;
-  const bool stars = D == 0u || (r >= 1u && 2u * r <= D);
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const uint32_t n = min(b->n_items, b->item_cap);
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
@@ -176,7 +171,6 @@ __global__ void __launch_bounds__(256, 4) k_bs_relax(BsCtx* b, DevGraph G) {
     const uint32_t v = item.x, chunk = item.y;
     uint32_t m = 0;
     if (mine) m = (__ldcg(&b->am[(uint64_t)v * Wm + (s >> 2)]) >> ((s & 3u) * 8u)) & 0xFFu;
-    const bool dostar = chunk == 0 && stars;
     uint32_t dv[8];
 #pragma unroll
     for (int i = 0; i < 8; i++) dv[i] = COST_INF;
@@ -184,7 +178,7 @@ __global__ void __launch_bounds__(256, 4) k_bs_relax(BsCtx* b, DevGraph G) {
 #pragma unroll
       for (int i = 0; i < 8; i++)
         if ((m >> i) & 1u) dv[i] = 0u;  // round 0: the members themselves
-    } else if (mine && (m || dostar)) {
+    } else if (mine && m) {
       const uint4* src = (const uint4*)&src_tab[(uint64_t)v * Gp + s * 8];
       const uint4 a = __ldcg(src), c4 = __ldcg(src + 1);
       dv[0] = a.x;
@@ -195,20 +189,6 @@ __global__ void __launch_bounds__(256, 4) k_bs_relax(BsCtx* b, DevGraph G) {
       dv[5] = c4.y;
       dv[6] = c4.z;
       dv[7] = c4.w;
-    }
-    if (dostar) {
-      // stars of every query at v (v's row in shared memory, one query per lane)
-      if (mine) {
-#pragma unroll
-        for (int i = 0; i < 8; i++) s_row[wib][s * 8 + i] = dv[i];
-      }
-      __syncwarp();
-      for (uint32_t q = (uint32_t)lane; q < nq; q += 32) {
-        uint64_t sum = 0;
-        for (uint32_t i = 0; i < b->qk[q]; i++) sum += s_row[wib][b->qcol[q][i]];
-        if (sum < (uint64_t)s_star[q]) atomicMin(&s_star[q], (uint32_t)sum);
-      }
-      __syncwarp();
     }
     // per active column: the heaviest edge it may still take from v (0: none; edge
     // weights are at least 1), and for the warp the heaviest of them all
@@ -299,9 +279,6 @@ __global__ void __launch_bounds__(256, 4) k_bs_relax(BsCtx* b, DevGraph G) {
   any = __reduce_or_sync(0xffffffffu, any);
   if (lane == 0 && any) b->ann = 1u;
   if (lane == 0 && relaxed) atomicAdd(&b->st_relax, relaxed);  // the same in every lane
-  __syncthreads();
-  for (uint32_t q = threadIdx.x; q < nq; q += blockDim.x)
-    if (s_star[q] < COST_INF) atomicMin(&b->star[q], s_star[q]);
 }
 
 // Hop-bounded tables (n4 = V x Gp / 4 uint4 per table).  Before round r >= 1:
@@ -329,9 +306,63 @@ __global__ void k_bs_copy(BsCtx* b, int64_t n4, int finish) {
   }
 }
 
-// Control (one block): column cutoffs from the query stars; the next step's buffers; the
-// end of the search.
-__global__ void k_bs_ctrl(BsCtx* b) {
+// Stars, before the relax step: at every vertex announced for this step (the first
+// chunk of its items), each query's columns summed (the query's k shortest paths from v
+// form a connected subgraph covering every group, a feasible cost).  Hop-bounded: from
+// table r with 2r <= D only (a tree of diameter <= D).  Found before the relax step, a
+// star lowers the cutoffs that this very step relaxes against.
+__global__ void __launch_bounds__(256) k_bs_star(BsCtx* b) {
+  __shared__ __align__(16) uint32_t s_row[256 / 32][BS_COLS];  // per warp: the vertex's row
+  __shared__ uint32_t s_star[BS_MAXQ];
+  if (b->done) return;
+  const uint32_t D = b->D, r = b->round;
+  if (D && !(r >= 1u && 2u * r <= D)) return;
+  const uint32_t* src_tab = D ? b->tab[r] : b->dist;
+  const uint32_t Gp = b->Gp, nsec = Gp / 8u, nq = b->nq;
+  for (uint32_t q = threadIdx.x; q < BS_MAXQ; q += blockDim.x) s_star[q] = COST_INF;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const uint32_t n = min(b->n_items, b->item_cap);
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  for (uint32_t base = wid * 32u; base < n; base += warps * 32u) {
+    // lane i looks at item base + i; the warp then takes the first chunks one by one
+    uint32_t v = 0;
+    bool first = false;
+    if (base + lane < n) {
+      const uint2 item = b->items[base + lane];
+      v = item.x;
+      first = item.y == 0u;
+    }
+    uint32_t todo = __ballot_sync(0xffffffffu, first);
+    while (todo) {
+      const int src = __ffs(todo) - 1;
+      todo &= todo - 1u;
+      const uint32_t x = __shfl_sync(0xffffffffu, v, src);
+      if ((uint32_t)lane < nsec) {
+        const uint4* p = (const uint4*)&src_tab[(uint64_t)x * Gp + lane * 8];
+        const uint4 a = __ldcg(p), c4 = __ldcg(p + 1);
+        uint4* o = (uint4*)&s_row[wib][lane * 8];
+        o[0] = a;
+        o[1] = c4;
+      }
+      __syncwarp();
+      for (uint32_t q = (uint32_t)lane; q < nq; q += 32) {
+        uint64_t sum = 0;
+        for (uint32_t i = 0; i < b->qk[q]; i++) sum += s_row[wib][b->qcol[q][i]];
+        if (sum < (uint64_t)s_star[q]) atomicMin(&s_star[q], (uint32_t)sum);
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  for (uint32_t q = threadIdx.x; q < nq; q += blockDim.x)
+    if (s_star[q] < COST_INF) atomicMin(&b->star[q], s_star[q]);
+}
+
+// Control (one block): column cutoffs from the query stars; with `advance`, after the
+// relax step, the next step's buffers and the end of the search.
+__global__ void k_bs_ctrl(BsCtx* b, int advance) {
   if (b->done) return;
   const uint32_t nq = b->nq, Gp = b->Gp;
   for (uint32_t c = threadIdx.x; c < Gp; c += blockDim.x) {
@@ -347,6 +378,7 @@ __global__ void k_bs_ctrl(BsCtx* b) {
         }
     if (used) b->cutc[c] = min(b->cutc[c], mx);
   }
+  if (!advance) return;
   __syncthreads();
   if (threadIdx.x == 0) {
     if (b->error || !b->ann) {

@@ -887,12 +887,14 @@ struct Runner {
           launches++;
         }
         k_bs_scan<<<eng->sms * 4, 256, 0, st>>>(d_b, G);
+        k_bs_star<<<eng->sms * 4, 256, 0, st>>>(d_b);
+        k_bs_ctrl<<<1, 256, 0, st>>>(d_b, 0);
         const int pe = prof_begin(PROF_BSRELAX);
         k_bs_relax<<<relax_blocks, 256, 0, st>>>(d_b, G);
         prof_end(pe);
         relax_launches++;
-        k_bs_ctrl<<<1, 256, 0, st>>>(d_b);
-        launches += 3;
+        k_bs_ctrl<<<1, 256, 0, st>>>(d_b, 1);
+        launches += 5;
       }
       CK(cudaGetLastError());
       CK(cudaMemcpyAsync(&hb, d_b, sizeof(BsCtx), cudaMemcpyDeviceToHost, st));
