@@ -625,7 +625,7 @@ def run_ours(args):
     if rank == 0:
         per_q, per_q_host = one_at_a_time([(queries[i], hops[i]) for i in timed[: args.single]])
 
-    # the north star's two query sizes on their own: batches of k = 5 only and k = 7 only
+    # the two headline query sizes on their own: batches of k = 5 only and k = 7 only
     # (the workload's queries of that size, in stream order), batched and one at a time
     by_k = {}
     if rank == 0 and not args.no_by_k:

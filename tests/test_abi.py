@@ -48,3 +48,26 @@ def test_binding_covers_engine_symbols():
     lib = C.CDLL(G.LIB_PATH)
     for n in G.C_ABI_SYMBOLS:
         assert hasattr(lib, n), n
+
+
+def test_build_tracks_every_device_header():
+    """A kernel edited in any csrc header rebuilds the library (every .cuh is a
+    dependency of the CUDA sources), so a stale library is never tested or timed."""
+    import build
+    csrc = os.path.join(os.path.dirname(G.__file__), "csrc")
+    cuh = sorted(f for f in os.listdir(csrc) if f.endswith(".cuh"))
+    assert cuh and set(cuh) <= set(build.HEADERS), (cuh, build.HEADERS)
+    lib = G.LIB_PATH
+    deps = [os.path.join(csrc, f) for f in cuh]
+    assert not build._stale(lib, deps) or not os.path.exists(lib)
+
+
+def test_stats_layout_matches_header():
+    """gst_stats in include/gst.h and the binding's Stats list the same fields in order."""
+    with open(os.path.join(INC, "gst.h")) as f:
+        src = f.read()
+    body = src[src.index("typedef struct gst_stats"):]
+    body = body[:body.index("} gst_stats;")]
+    body = re.sub(r"/\*.*?\*/", " ", body, flags=re.S)
+    fields = re.findall(r"(?:int64_t|double|int32_t)\s+(\w+);", body)
+    assert fields == [n for n, _ in G.Stats._fields_]
