@@ -1162,6 +1162,12 @@ __global__ void __launch_bounds__(256, 4) k_rows(Ctx* ctxs, int nctx, DevGraph G
     if (!in_bounds(c, v < G.V && c->RW <= rw_max, 8)) continue;
     const int RW = c->RW, W = c->W, DD = c->DD, k = c->k, D = c->D, hop = c->hop;
     (void)W;
+    // cell i sits at i ^ ((i >> 4) & swz) in shared memory: the partners of a merge round
+    // (submasks of one complement, cells of one popcount class) often share their low
+    // index bits, and the XOR spreads them over the banks; a row whose width is not a
+    // multiple of 16 cells stays unswizzled (its positions must stay below RW)
+    const uint32_t swz = (RW & 15) ? 0u : 15u;
+    auto B = [&](uint32_t i) -> unsigned long long& { return buf[i ^ ((i >> 4) & swz)]; };
     const uint32_t full = (uint32_t)c->full;
     unsigned long long* row = (unsigned long long*)row_of(c, v);
     if (row == nullptr) {  // never for a dirty row: a row is taken before its first write
@@ -1178,7 +1184,7 @@ __global__ void __launch_bounds__(256, 4) k_rows(Ctx* ctxs, int nctx, DevGraph G
       uint64_t x = CELL_INF;
       if (i < RW) {
         x = __ldcg(row + i);
-        buf[i] = x;
+        B((uint32_t)i) = x;
       }
       // an unreached cell is all ones, so its pending bit must be ignored
       const bool fin = i < RW && x != CELL_INF;
@@ -1258,9 +1264,9 @@ __global__ void __launch_bounds__(256, 4) k_rows(Ctx* ctxs, int nctx, DevGraph G
             Y = __ldg(&SUBMASK.v[full ^ X][r - d2 * m + 1u]);
           }
           const uint32_t yi = (d2 << k) + Y;
-          const uint32_t cy = (Y & X) ? COST_INF : cost_of(buf[yi]);
+          const uint32_t cy = (Y & X) ? COST_INF : cost_of(B(yi));
           const uint32_t S = X | Y;
-          const uint32_t cand = cost_of(buf[cell]) + cy;
+          const uint32_t cand = cost_of(B(cell)) + cy;
           bool ok = cy != COST_INF && !(hop && (int)(d1 + d2) > D) &&
                     in_bounds(c, yi < (uint32_t)RW && S < (uint32_t)W, 9);
           if (ok && S != full && 3ull * cand > 2ull * ubm) ok = false;
@@ -1268,8 +1274,8 @@ __global__ void __launch_bounds__(256, 4) k_rows(Ctx* ctxs, int nctx, DevGraph G
             const uint32_t nd = d1 > d2 ? d1 : d2;
             tgt = (nd << k) + S;
             const uint64_t nv = pack_cell(cand, PEND | MERGE | Y | (d2 << 16) | (d1 << 21));
-            if (nv < buf[tgt]) {
-              const uint64_t old = atomicMin(&buf[tgt], (unsigned long long)nv);
+            if (nv < B(tgt)) {
+              const uint64_t old = atomicMin(&B(tgt), (unsigned long long)nv);
               if (nv < old) {
                 newf = old == CELL_INF;
                 const uint32_t bit = 1u << (tgt & 31);
@@ -1335,7 +1341,7 @@ __global__ void __launch_bounds__(256, 4) k_rows(Ctx* ctxs, int nctx, DevGraph G
         for (int b = 0; b < KMAX; b++) dl[b] = hb[b];
       }
       if (i < RW && ((pend[i >> 5] >> (i & 31)) & 1u)) {
-        const uint64_t x = buf[i];
+        const uint64_t x = B((uint32_t)i);
         row[i] = x & ~(uint64_t)PEND;
         const uint32_t cst = cost_of(x);
         const uint32_t p = (uint32_t)i & full, d = (uint32_t)i >> k;
@@ -1396,7 +1402,7 @@ __global__ void __launch_bounds__(256, 4) k_rows(Ctx* ctxs, int nctx, DevGraph G
         }
         if (t < ncand) {
           const uint32_t i = list[t];
-          const uint32_t p = i & full, cst = cost_of(buf[i]);
+          const uint32_t p = i & full, cst = cost_of(B(i));
           const uint32_t Xb = full ^ p;
           const uint32_t* W2 = tour + (size_t)Wq * TOUR_STRIDE + (size_t)Xb * KMAX;
           uint32_t mind = COST_INF;
@@ -1443,7 +1449,7 @@ __global__ void __launch_bounds__(256, 4) k_rows(Ctx* ctxs, int nctx, DevGraph G
       for (int i0 = 0; i0 < RW; i0 += 32) {
         const int i = i0 + lane;
         if (i < RW && ((pend[i >> 5] >> (i & 31)) & 1u)) {
-          const uint32_t key = cost_of(buf[i]) + 1u;
+          const uint32_t key = cost_of(B(i)) + 1u;
           if (key >= bend) {
             cf++;
             kmin = min(kmin, key);
@@ -1471,7 +1477,7 @@ __global__ void __launch_bounds__(256, 4) k_rows(Ctx* ctxs, int nctx, DevGraph G
         for (int i0 = 0; i0 < RW; i0 += 32) {
           const int i = i0 + lane;
           if (i < RW && ((pend[i >> 5] >> (i & 31)) & 1u)) {
-            const uint32_t cst = cost_of(buf[i]);
+            const uint32_t cst = cost_of(B(i));
             const uint32_t p = (uint32_t)i & full, d = (uint32_t)i >> k;
             const uint4 item = make_uint4(v, p | (d << 16), cst, 0u);
             if (cst + 1u >= bend) {
