@@ -1703,6 +1703,17 @@ int shared_kind(const Runner& R, const Job* j) {
   return D < 0 ? 0 : D;
 }
 
+// Groups of job j in the group cache of its kind.
+int cached_groups(const Runner& R, const Job* j) {
+  const int D = j->q.hop_bound;
+  const auto& hc = R.grp->hop_cache;
+  int n = 0;
+  for (int i = 0; i < j->q.k; i++)
+    n += D < 0 ? R.grp->cache.vec(j->gids[i]) != nullptr
+               : hc.cap > 0 && hc.D == D && hc.vec(j->gids[i]) != nullptr;
+  return n;
+}
+
 // One shared search over the first waiting queries of one kind (0 unbounded, else D).
 gst_status shared_search_kind(Runner& R, std::deque<Job*>& pending, int kind) {
   std::vector<Job*> chunk;
@@ -1717,14 +1728,18 @@ gst_status shared_search_kind(Runner& R, std::deque<Job*>& pending, int kind) {
       if (std::find(cols.begin(), cols.end(), j->gids[i]) == cols.end()) cols.push_back(j->gids[i]);
     chunk.push_back(j);
   }
-  if (chunk.size() < 2) return GST_OK;
+  // a lone query with cached groups searches on its own: its search then covers only
+  // the other groups, and its star counts the cached distances from the start
+  if (chunk.empty() || (chunk.size() == 1 && cached_groups(R, chunk[0]) > 0)) return GST_OK;
   return R.shared_search(chunk, cols, kind);
 }
 
 // Before admitting: for every kind (unbounded, or one hop bound D) with no shared table
-// pending and at least two eligible queries waiting, search their groups together (the
-// first queries of that kind in order, up to BS_COLS distinct groups and BS_MAXQ
-// queries).  Kinds are searched in the order their first queries wait.
+// pending and an eligible query waiting, search the groups of that kind's first
+// queries together (in order, up to BS_COLS distinct groups and BS_MAXQ queries).  A
+// lone query takes the same path: its search over k columns on these kernels is faster
+// than the per-query group-mask search on large graphs.  Kinds are searched in the
+// order their first queries wait.
 gst_status maybe_shared_search(Runner& R, std::deque<Job*>& pending) {
   if (!R.eng->cfg.batch_search) return GST_OK;
   R.shared_release(false);

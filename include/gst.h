@@ -81,10 +81,13 @@ typedef struct gst_config {
                                  bounds to the DP (the autotuner chooses it) */
   int32_t hop_cut_permille;   /* hop-bounded queries: the same in thousandths (0: use
                                  hop_cut_mult x 1000) */
-  int32_t batch_search;       /* 1 (default): gst_solve_batch searches the distances of its
-                                 unbounded queries' groups together, up to 256 groups at a
-                                 time (one relaxation of an edge serves every group that
-                                 improved at its source); 0: every query searches alone */
+  int32_t batch_search;       /* 1 (default): gst_solve, gst_solve_batch and the server
+                                 search the distances of their waiting queries' groups
+                                 together, one search per kind (unbounded, or one hop bound
+                                 <= 8), up to 256 groups and 64 queries at a time (one
+                                 relaxation of an edge serves every group that improved at
+                                 its source; a lone query runs the same kernels); 0: every
+                                 query runs its own group-mask search */
 } gst_config;
 
 typedef struct gst_query {

@@ -282,8 +282,9 @@ def test_search_cutoff_keeps_optima(permille):
 def test_shared_search_matches_alone(engine):
     """The queries of a batch search their groups' distances together, one search per
     kind (unbounded, or one hop bound D: D tables of paths of at most 1..D edges), at most
-    256 groups and 64 queries per search: every optimum equals the query solved alone and
-    the oracle's, and the trees verify."""
+    256 groups and 64 queries per search, and a lone query runs the same kernels: every
+    optimum equals the query solved alone with its own group-mask search and the
+    oracle's, and the trees verify."""
     rng = np.random.default_rng(61)
     g = G.synth_rmat(3000, 14000, 62)
     grp = G.synth_groups_zipf(g.V, 400, 1.5, 1, 60, 63)
@@ -293,9 +294,22 @@ def test_shared_search_matches_alone(engine):
         k = int(rng.integers(2, 7))
         qs.append(rng.choice(grp.n_groups, size=k, replace=False).astype(np.int32))
         hops.append(kinds[t % len(kinds)])
+    # alone: every query with its own group-mask search (the shared search off)
+    own = G.Engine(0, batch_search=0)
+    dgo = own.graph(g, grp)
+    try:
+        alone = [dgo.solve(q, h) for q, h in zip(qs, hops)]
+        assert all(a.stats["shared_launches"] == 0 for a in alone)
+    finally:
+        dgo.close()
+        own.close()
     dg = engine.graph(g, grp)
     try:
-        alone = [dg.solve(q, h) for q, h in zip(qs, hops)]
+        # a lone query runs the shared kernels too, with its own cutoff
+        lone = [dg.solve(q, h) for q, h in list(zip(qs, hops))[:21]]
+        assert all(a.stats["shared_launches"] > 0 for a in lone)
+        for a, b in zip(alone, lone):
+            assert a.status == b.status and (not a.ok or a.cost == b.cost), (a.cost, b.cost)
         mixed = dg.solve_batch(qs, hops)
         assert mixed[0].stats["shared_launches"] > 0
         for q, h, a, b in zip(qs, hops, alone, mixed):
