@@ -1703,17 +1703,6 @@ int shared_kind(const Runner& R, const Job* j) {
   return D < 0 ? 0 : D;
 }
 
-// Groups of job j in the group cache of its kind.
-int cached_groups(const Runner& R, const Job* j) {
-  const int D = j->q.hop_bound;
-  const auto& hc = R.grp->hop_cache;
-  int n = 0;
-  for (int i = 0; i < j->q.k; i++)
-    n += D < 0 ? R.grp->cache.vec(j->gids[i]) != nullptr
-               : hc.cap > 0 && hc.D == D && hc.vec(j->gids[i]) != nullptr;
-  return n;
-}
-
 // One shared search over the first waiting queries of one kind (0 unbounded, else D).
 gst_status shared_search_kind(Runner& R, std::deque<Job*>& pending, int kind) {
   std::vector<Job*> chunk;
@@ -1728,9 +1717,7 @@ gst_status shared_search_kind(Runner& R, std::deque<Job*>& pending, int kind) {
       if (std::find(cols.begin(), cols.end(), j->gids[i]) == cols.end()) cols.push_back(j->gids[i]);
     chunk.push_back(j);
   }
-  // a lone query with cached groups searches on its own: its search then covers only
-  // the other groups, and its star counts the cached distances from the start
-  if (chunk.empty() || (chunk.size() == 1 && cached_groups(R, chunk[0]) > 0)) return GST_OK;
+  if (chunk.empty()) return GST_OK;
   return R.shared_search(chunk, cols, kind);
 }
 
