@@ -1273,12 +1273,9 @@ struct gst_server {
   int64_t admitted = 0, completed = 0;
 };
 
-// defined with the batch driver below (inside its extern "C" block)
-extern "C" {
 namespace {
-gst_status maybe_shared_search(Runner& R, std::deque<Job*>& pending);
+gst_status maybe_shared_search(Runner& R, std::deque<Job*>& pending);  // with the batch driver
 }  // namespace
-}  // extern "C"
 
 namespace {
 
@@ -1680,6 +1677,8 @@ gst_status gst_groups_destroy(gst_groups* gr) {
   return GST_OK;
 }
 
+}  // extern "C"
+
 namespace {
 // Run the pending jobs on R with at most B resident (admitting beyond the batch size
 // would change it), refilling slots as queries finish; capacity overflows are re-run
@@ -1808,6 +1807,10 @@ gst_status batch_runner(gst_graph* g, int B) {
 }
 }  // namespace
 
+extern "C" {
+
+}  // extern "C"
+
 namespace {
 // Warm cache C of groups grp for hop bound D (-1: unlimited distances): see
 // gst_groups_cache_warm / gst_groups_cache_warm_hop.  Caller holds the engine lock.
@@ -1901,6 +1904,8 @@ gst_status cache_warm(gst_groups* grp, gst_groups::Cache& C, int32_t D, int32_t 
   return GST_OK;
 }
 }  // namespace
+
+extern "C" {
 
 gst_status gst_groups_cache_warm(gst_groups* grp, int32_t n, const int32_t* group_ids,
                                  int64_t max_bytes, int32_t* n_cached) {
@@ -2067,6 +2072,8 @@ void gst_result_free(gst_result* r) {
 // cached as one line per shape in a text file, so later runs on a graph of the same
 // shape skip the search.
 
+}  // extern "C"
+
 namespace {
 
 std::string shape_key(const gst_graph* g, int32_t max_batch) {
@@ -2118,6 +2125,8 @@ bool read_cache(const char* path, const std::string& key, TuneParams* p) {
 }
 
 }  // namespace
+
+extern "C" {
 
 extern "C" gst_status gst_autotune(gst_graph* g, gst_groups* grp, int32_t n,
                                    const gst_query* sample, const char* cache_path,
