@@ -41,7 +41,7 @@
 namespace gst {
 
 constexpr int BS_COLS = 256;   // columns (distinct groups) of one shared search, at most
-constexpr int BS_CHUNK = 64;   // edges per relax item
+constexpr int BS_CHUNK = 128;  // edges per relax item
 constexpr int BS_MAXQ = MAXB;  // queries of one shared search, at most
 
 struct BsCtx {
